@@ -1,0 +1,363 @@
+"""Benchmark of the batched cut-scoring hot path (one JSON line on rank 0).
+
+Workload: dense unweighted MAXCUT, Erdos-Renyi G(n=2048, p=0.5), unit weights,
+dense symmetric float32 couplings with a zero diagonal (seeded synthetic, the
+shape of the named configuration); 4096 candidate bit strings per batch
+(seeded uniform bits), scored as the reference's calculate_cut does
+(kernels.cl:44-94) and selected with its tie rule. One step = one batch.
+
+* value: candidates scored per second over all ranks (cut evals/s), device time
+  of the timed steps (CUDA events), inputs already in HBM. L2 is flushed
+  (a 256 MB write) between timed steps, outside the timed windows.
+* e2e: the same metric through the public path with host buffers: each step
+  copies the packed batch from pinned host memory, scores it through the C ABI
+  and reads the (best value, index) pair back.
+* roofline: the scoring GEMM (2*B*n^2 integer ops per launch) against the
+  int8 tensor rate, taken as twice the measured dense bf16 rate.
+* cpu_baseline: the oracle's C port of the reference's cut_worker on the
+  host cores (a bounded sample of the batch).
+
+Multi-GPU: every rank scores its own batches (weak scaling); the only
+exchange is the max over ranks of the elapsed time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+N_NODES = 2048
+BATCH = 4096
+EDGE_P = 0.5
+METRIC = "cut evals/s"
+UNIT = "candidates/s"
+
+
+def workload_config(extra=None):
+    cfg = {
+        "workload": "ER G(n=2048,p=0.5) unit weights, 4096 candidates per batch, calculate_cut + reference-order argmax",
+        "n": N_NODES,
+        "batch": BATCH,
+        "weights": "int8 (exact)",
+        "l2": "flushed between timed steps (256 MB write)",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), float(p["bf16_tflops"]), "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks sampled every 200 ms while the timed region runs."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def __enter__(self):
+        try:
+            self._proc = subprocess.Popen(
+                [
+                    "nvidia-smi",
+                    f"--id={self.index}",
+                    "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                    "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                    "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                    "--format=csv,noheader,nounits",
+                    "-lms",
+                    "200",
+                ],
+                stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL,
+                text=True,
+            )
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+
+    def summary(self):
+        sm = [float(s[0]) for s in self.samples if len(s) >= 7 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 7 and s[1].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            if len(s) >= 7:
+                for nm, v in zip(names, s[3:7]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        return {
+            "sm_mhz": float(np.median(sm)) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons),
+            "samples": len(self.samples),
+        }
+
+
+def cpu_baseline(W, X, spin=False, sample=256, max_seconds=20.0):
+    """Oracle C port of cut_worker over a sample of the batch, all host threads."""
+    from oracle import oracle as O
+
+    O.build_oracle()
+    cores = os.cpu_count() or 1
+    th = O.pack32(X[:sample])
+    O.cut_values(W, th[:8], 8, spin)  # warm
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        O.cut_values(W, th, sample, spin)
+        done += sample
+        if time.perf_counter() - t0 > min(max_seconds, 2.0) or done >= 4 * sample:
+            break
+    dt = time.perf_counter() - t0
+    return {
+        "value": done / dt,
+        "unit": UNIT,
+        "cores": cores,
+        "kind": "port",
+        "sample": f"{done} candidates of n={W.shape[0]} scored by the oracle's C port of cut_worker (OpenMP over candidates)",
+    }
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    W = make_graph()
+    X = make_batch(0)
+    t_steps = []
+    from oracle import oracle as O
+
+    O.build_oracle()
+    cores = os.cpu_count() or 1
+    sample = 512
+    th = O.pack32(X[:sample])
+    for _ in range(max(1, args.warmup)):
+        O.cut_values(W, th[:64], 64, 0)
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        vals = O.cut_values(W, th, sample, 0)
+        O.select(vals, *O.cut_geometry(sample, 148))
+        t_steps.append(time.perf_counter() - t0)
+    ms = 1000.0 * float(np.mean(t_steps))
+    value = sample / (ms / 1000.0)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": workload_config({"reference_sample": f"{sample} of the {BATCH} candidates per step"}),
+        "cpu_baseline": {
+            "value": value,
+            "unit": UNIT,
+            "cores": cores,
+            "kind": "port",
+            "sample": f"{sample} candidates per step, oracle C port of calculate_cut (kernels.cl:44-94) + its selection, OpenMP over candidates",
+        },
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def make_graph():
+    from pyqrackising_b200 import workloads as wl
+
+    return wl.erdos_renyi(N_NODES, EDGE_P, seed=1)
+
+
+def make_batch(seed):
+    return np.random.default_rng(1000 + seed).random((BATCH, N_NODES)) < 0.5
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = dist_mod
+
+    from oracle import oracle as O
+    from pyqrackising_b200 import _lib
+    from pyqrackising_b200.device import DeviceGraph
+
+    W = make_graph()
+    dg = DeviceGraph(W)
+    G, L = O.cut_geometry(BATCH, 148)
+    nb = 4
+    batches_host = [O.pack32(make_batch(rank * 97 + i)) for i in range(nb)]
+    batches = [torch.from_numpy(b.view(np.int32).reshape(-1)).to(dg.device) for b in batches_host]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dg.device)
+    stream = torch.cuda.current_stream()
+
+    # correctness spot check against the oracle on a few candidates (outside timing)
+    e, be, bi = dg.calculate_cut(batches[0], BATCH, False, G, L)
+    ref = O.cut_values(W, batches_host[0][:16], 16, 0)
+    assert np.array_equal(e[:16].cpu().numpy(), ref), "scoring mismatch against the oracle"
+
+    for i in range(args.warmup):
+        dg.calculate_cut(batches[i % nb], BATCH, False, G, L, energies=False)
+    torch.cuda.synchronize()
+
+    # device-resident timing: events around each step, L2 flushed between steps
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clocks:
+        wall0 = time.perf_counter()
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            evs[i][0].record(stream)
+            dg.calculate_cut(batches[i % nb], BATCH, False, G, L, energies=False)
+            evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+        step_ms = [a.elapsed_time(b) for a, b in evs]
+        total_ms = float(np.sum(step_ms))
+
+        # e2e through the C ABI with host buffers (pinned), copies inside the window
+        pinned = [torch.from_numpy(b.view(np.int32).reshape(-1)).pin_memory() for b in batches_host]
+        dev_in = torch.empty_like(batches[0])
+        out_e = torch.empty(1, dtype=torch.float32).pin_memory()
+        out_i = torch.empty(1, dtype=torch.int32).pin_memory()
+        e2e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        for i in range(args.warmup):
+            dev_in.copy_(pinned[i % nb], non_blocking=True)
+            _, be, bi = dg.calculate_cut(dev_in, BATCH, False, G, L, energies=False)
+            out_e.copy_(be, non_blocking=True)
+            out_i.copy_(bi, non_blocking=True)
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            flush.fill_(i & 0xFF)
+            e2e_evs[i][0].record(stream)
+            dev_in.copy_(pinned[i % nb], non_blocking=True)
+            _, be, bi = dg.calculate_cut(dev_in, BATCH, False, G, L, energies=False)
+            out_e.copy_(be, non_blocking=True)
+            out_i.copy_(bi, non_blocking=True)
+            e2e_evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = float(np.sum([a.elapsed_time(b) for a, b in e2e_evs]))
+
+    if dist:
+        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dg.device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_ms = float(t[0]), float(t[1])
+
+    ms_per_step = total_ms / args.steps
+    value = world * BATCH * args.steps / (total_ms / 1000.0)
+    e2e_value = world * BATCH * args.steps / (e2e_ms / 1000.0)
+    hbm, bf16, src = peaks()
+    ops = 2.0 * BATCH * N_NODES * N_NODES
+    achieved = ops / (ms_per_step / 1000.0) / 1e12
+    int8_peak = 2.0 * bf16
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int8" if dg.is_integer else "bf16x2",
+        "data": "synthetic",
+        "config": workload_config(),
+        "e2e": {
+            "value": e2e_value,
+            "unit": UNIT,
+            "h2d_bytes_per_step": int(batches_host[0].nbytes),
+            "d2h_bytes_per_step": 8,
+        },
+        "roofline": {
+            "bound": "tensor",
+            "achieved": achieved,
+            "peak": int8_peak,
+            "unit": "TOPS",
+            "frac": achieved / int8_peak,
+            "traffic": None,
+            "peak_basis": f"int8 dense = 2 x bf16 dense ({src} bf16 {bf16} TFLOP/s)",
+            "kernel": "pqi_calculate_cut (scoring GEMM + finish + select)",
+            "algorithmic_ops_per_launch": ops,
+        },
+        "gpu_launches": 3 * args.steps,
+        "wall_s_timed_loop": wall,
+    }
+    if rank == 0:
+        line["clocks"] = clocks.summary()
+        if world == 1:
+            try:
+                line["cpu_baseline"] = cpu_baseline(W, make_batch(0))
+            except Exception as ex:  # pragma: no cover
+                line["cpu_baseline"] = {"unavailable": str(ex)}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

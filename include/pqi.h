@@ -1,0 +1,277 @@
+/*
+ * pqi.h - C ABI of libpqi, the B200 (sm_100a) implementation of PyQrackIsing's
+ * dense cut-scoring and local-search path.
+ *
+ * Conventions
+ *  - Every pointer argument is DEVICE memory owned by the caller unless the
+ *    name ends in _host. The library never allocates or frees device memory;
+ *    calls that need scratch take a caller-provided workspace whose size is
+ *    given by pqi_workspace_bytes().
+ *  - Every entry point returns a pqi_status. Launch errors are reported as
+ *    PQI_ECUDA; a device-side iteration budget that runs out is PQI_ETIMEOUT.
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream). Calls are
+ *    asynchronous on that stream unless documented otherwise.
+ *  - Bit strings use the reference's layout: node j is bit (j & 31) of
+ *    32-bit word (j >> 5) (pyqrackising/maxcut_tfim_util.py:304-316), or bit
+ *    (j & 63) of 64-bit word (j >> 6) for the gray search (util:290-301).
+ *  - Selection ("argmax") follows the reference's launch geometry
+ *    (global_size G, local_size L as setup_opencl computes them,
+ *    maxcut_tfim_util.py:169-221) so ties resolve to the same index as the
+ *    reference: first maximum within each work-item's grid-stride sequence
+ *    (kernels.cl:78-91), then the work-group halving tree of
+ *    reduce_energy_index (kernels.cl:1-29), then the first group
+ *    (np.argmax, spin_glass_solver.py:211). L must be <= 64 and divide G.
+ */
+#ifndef PQI_H
+#define PQI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  PQI_OK = 0,
+  PQI_EINVAL = 1,   /* bad argument: size, geometry, null pointer, unsupported weights */
+  PQI_ECUDA = 2,    /* a CUDA launch or runtime call failed */
+  PQI_ETIMEOUT = 3, /* a device-side iteration budget ran out; outputs are partial */
+  PQI_ENOTSUP = 4   /* the device is not sm_100 or a feature is unavailable */
+} pqi_status;
+
+/* Storage chosen for the coupling matrix by pqi_prepare_weights. */
+typedef enum {
+  PQI_W_F32 = 0,  /* float32 only (non-integer weights) plus bf16 hi/lo split */
+  PQI_W_I8 = 1    /* integer weights in [-127, 127]: exact int8 copy */
+} pqi_wkind;
+
+/*
+ * Device-resident coupling matrix. W is n x n float32 row-major, symmetric,
+ * as nx.to_numpy_array produces it (spin_glass_solver.py:458-461). The
+ * prepared copies have a zero diagonal (the reference's kernels never read
+ * the diagonal: kernels.cl:44-62, 100-116, 150-184). ld is the row pitch of
+ * the prepared copies in elements (n rounded up to a multiple of 128), so
+ * every prepared row starts on a 512-byte boundary.
+ */
+typedef struct {
+  const float* W;        /* n*n float32, caller's matrix (diagonal as given) */
+  const int8_t* W_i8;    /* n*ld int8 (PQI_W_I8), zero padded, else NULL */
+  const uint16_t* W_hi;  /* n*ld bf16 bits (PQI_W_F32), zero padded, else NULL */
+  const uint16_t* W_lo;  /* n*ld bf16 bits of W - hi (PQI_W_F32), else NULL */
+  const float* W_f32z;   /* n*ld float32 with zero diagonal, zero padded */
+  int n;
+  int ld;
+  int kind;              /* pqi_wkind */
+  double upper_sum;      /* sum_{u<v} W_uv (host value, filled by pqi_prepare_weights) */
+} pqi_weights;
+
+/* ---------------------------------------------------------------------------
+ * Set-up
+ * -------------------------------------------------------------------------*/
+
+/* Version string of the library build. */
+const char* pqi_version(void);
+
+/* Text of the last CUDA error the calling host thread saw inside the library. */
+const char* pqi_last_error(void);
+
+/* PQI_OK when device `device` is an sm_100 part the library was built for. */
+pqi_status pqi_check_device(int device);
+
+/* Bytes of workspace any entry point needs for a problem of n nodes and up
+ * to `count` candidates / seeds. A workspace of this size serves every call. */
+size_t pqi_workspace_bytes(int n, long count);
+
+/* Row pitch (elements) of the prepared copies of an n-node matrix: W_f32z is
+ * n*ld floats, W_i8 n*ld bytes, W_hi/W_lo n*ld bf16 each. */
+int pqi_padded_ld(int n);
+
+/* Result of pqi_scan_weights (host struct). */
+typedef struct {
+  unsigned long long nonfinite; /* NaN/Inf entries */
+  unsigned long long nonint;    /* off-diagonal entries that are not integers */
+  unsigned long long asym;      /* (i, j) with W_ij != W_ji, each pair counted twice */
+  float maxabs;                 /* max |W_ij| off the diagonal */
+  int kind;                     /* pqi_wkind the prepared copies will use */
+  double upper_sum;             /* sum_{u<v} W_uv in float64 (fixed reduction order) */
+} pqi_weight_stats;
+
+/*
+ * Scan W once on the device: finite, integer-valued, symmetric, max |W| and
+ * the float64 sum of the upper triangle. Synchronises `stream` and fills
+ * *stats_host. Returns PQI_EINVAL for non-finite or asymmetric W (the
+ * reference's kernels read only the upper triangle for cuts but whole rows
+ * for flips, so they agree only on symmetric matrices).
+ */
+pqi_status pqi_scan_weights(const float* W, int n, void* workspace, size_t workspace_bytes,
+                            pqi_weight_stats* stats_host, void* stream);
+
+/*
+ * Build the prepared copies chosen by stats->kind: W_f32z always, W_i8 for
+ * PQI_W_I8 (every off-diagonal weight an integer in [-127, 127]), W_hi/W_lo
+ * for PQI_W_F32. Pointers of the copies not needed may be NULL. Fills
+ * *out_host. Replaces make_G_m_buf (maxcut_tfim_util.py:224-238).
+ */
+pqi_status pqi_prepare_weights(const float* W, int n, const pqi_weight_stats* stats_host,
+                               float* W_f32z, int8_t* W_i8, uint16_t* W_hi, uint16_t* W_lo,
+                               pqi_weights* out_host, void* stream);
+
+/* Select the batched-scoring implementation: 0 = tensor cores (tcgen05, the
+ * default), 1 = CUDA cores. Process-wide; used to cross-check the two. */
+pqi_status pqi_score_set_path(int path);
+
+/* ---------------------------------------------------------------------------
+ * Kernel-level replacements of the reference's OpenCL kernels
+ * -------------------------------------------------------------------------*/
+
+/*
+ * Batched cut scoring. theta: shots x ceil(n/32) words. Writes each
+ * candidate's value, as cut_worker defines it (kernels.cl:44-62: sum over
+ * u<v of W_uv if bits differ, else -W_uv when is_spin_glass, else 0), to
+ * energies (float32, nullable), and the selected (value, index) under
+ * geometry (G, L) to best_energy/best_index (device scalars). Integer
+ * weights run on the int8 tensor-core path with int32 accumulation (exact);
+ * float weights on the split-bf16 tensor-core path with fp32 accumulation.
+ * Replaces calculate_cut (kernels.cl:64-94) plus the host argmax of
+ * run_cut_opencl (maxcut_tfim.py:212-285).
+ */
+pqi_status pqi_calculate_cut(const pqi_weights* w, const uint32_t* theta, int shots,
+                             int is_spin_glass, int global_size, int local_size,
+                             float* energies, float* best_energy, int* best_index,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Single-flip gain vectors for `count` states: gains[b*n + k] = the cut change
+ * of flipping node k of state b, i.e. sum_{v != k} W_kv * (s_k == s_v ? 1 : -1)
+ * (single_bit_flip_worker, kernels.cl:100-116). float32 output; gains64
+ * (nullable) receives the same values accumulated in float64.
+ */
+pqi_status pqi_gains(const pqi_weights* w, const uint32_t* theta, int count, float* gains,
+                     double* gains64, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Selection over `count` float32 values under geometry (G, L); NaN never
+ * selected. Writes device scalars best_value/best_index.
+ * Replaces reduce_energy_index (kernels.cl:1-29) plus np.argmax over groups.
+ */
+pqi_status pqi_select(const float* values, long count, int global_size, int local_size,
+                      float* best_value, int* best_index, void* workspace,
+                      size_t workspace_bytes, void* stream);
+
+/*
+ * Host twin of pqi_select over host memory (no GPU needed): the same 64-bit
+ * key order, evaluated on the CPU. For callers that select on the host and
+ * for checking the key order against the reference's reduction.
+ */
+pqi_status pqi_select_host(const float* values_host, long count, int global_size, int local_size,
+                           float* best_value_host, int* best_index_host);
+
+/*
+ * One single-bit-flip pass: value_k = gain_k (x2 when is_spin_glass), selected
+ * under (G, L). Replaces single_bit_flips (kernels.cl:118-148).
+ */
+pqi_status pqi_single_bit_flips(const pqi_weights* w, const uint32_t* theta, int is_spin_glass,
+                                int global_size, int local_size, float* best_energy,
+                                int* best_index, void* workspace, size_t workspace_bytes,
+                                void* stream);
+
+/*
+ * One double-bit-flip pass over all pairs k < l in the reference's linear
+ * order c = k(n-1) - k(k-1)/2 + (l-k-1) (kernels.cl:206-218): value_c =
+ * g_k + g_l - 2 W_kl (s_k == s_l ? 1 : -1), x2 when is_spin_glass, which equals
+ * double_bit_flip_worker (kernels.cl:150-184). gains64 (nullable) are the
+ * float64 gains of theta from pqi_gains; when NULL they are computed here.
+ * best_index receives c. Replaces double_bit_flips (kernels.cl:186-231).
+ * n(n-1)/2 must fit in int32, as in the reference (n <= 46341).
+ */
+pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
+                                const double* gains64, int is_spin_glass, int global_size,
+                                int local_size, float* best_energy, int* best_index,
+                                void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Parallel Gray-code search of `seeds` perturbed copies of theta64
+ * (ceil(n/64) words), with the reference's schedule (gray kernel,
+ * kernels.cl:894-978): seed s starts from theta xor the seed mask of work-item
+ * s (kernels.cl:915-926, including its 32-bit shift), then for i = s, s+seeds,
+ * ... < iters_bound and every 64-node block b flips node ctz(i+1) + 64b and
+ * keeps the flip when it raises the cut. Flips landing on a node >= n are
+ * skipped (the reference reads outside W there). Writes theta_out
+ * (seeds x ceil(n/64) words) and energy_out (seeds floats: cut change of the
+ * seed's final state, halved when !is_spin_glass, as kernels.cl:974-976).
+ * gains64 (nullable): float64 gains of theta. Gains are kept per seed in
+ * shared memory and updated in O(n) per accepted flip instead of recomputed.
+ * Replaces gray (kernels.cl:894-978).
+ */
+pqi_status pqi_gray(const pqi_weights* w, const uint64_t* theta64, const double* gains64,
+                    int is_spin_glass, int iters_bound, int seeds, uint64_t* theta_out,
+                    float* energy_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Device-resident search (no host round trip per accepted move)
+ * -------------------------------------------------------------------------*/
+
+/*
+ * Repeats single-bit-flip passes on the device until no flip has positive
+ * value or max_flips flips were made: each step selects under (G, L) exactly
+ * as pqi_single_bit_flips and, if the value is > 0, flips that node and
+ * updates the gains in O(n). theta (in/out, ceil(n/32) words) and gains64
+ * (in/out, float64, from pqi_gains) stay on the device. Outputs (device):
+ * energy_sum (float64 sum of the accepted float32 values, what the
+ * reference adds to max_energy at spin_glass_solver.py:623-626), flips
+ * (int), and trace (nullable, max_flips ints: the flipped nodes in order).
+ * Returns PQI_ETIMEOUT when max_flips is reached with an improving flip left.
+ * Replaces the repeated single-flip iterations of the driver loop
+ * (spin_glass_solver.py:605-627).
+ */
+pqi_status pqi_single_descent(const pqi_weights* w, uint32_t* theta, double* gains64,
+                              int is_spin_glass, int global_size, int local_size, int max_flips,
+                              double* energy_sum, int* flips, int* trace, void* workspace,
+                              size_t workspace_bytes, void* stream);
+
+/* Flip nodes k (and l when l >= 0) of theta and update gains64 in O(n).
+ * Used after an accepted double flip or to apply a move chosen on the host. */
+pqi_status pqi_apply_flip(const pqi_weights* w, uint32_t* theta, double* gains64, int k, int l,
+                          void* stream);
+
+/*
+ * Exhaustive search over all 2^n states (1 <= n <= 30; the reference uses it
+ * for n < 24). W is the caller's n*n float32 matrix. Values are float64 sums in
+ * the reference's order: exact_maxcut sums W_ij over i<j with differing bits,
+ * exact_spin_glass sums +W_ij for equal bits and -W_ij otherwise
+ * (maxcut_tfim.py:288-339). Writes the reference's selection: the smallest
+ * mask attaining the maximum when that exceeds -1.0, else (mask 0, -1.0).
+ * best_value (double) and best_mask (int, bit i = node i) are device scalars.
+ */
+pqi_status pqi_exact_search(const float* W, int n, int is_spin_glass, double* best_value,
+                            int* best_mask, void* workspace, size_t workspace_bytes,
+                            void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Objectives, packing
+ * -------------------------------------------------------------------------*/
+
+/*
+ * float64 re-scoring of `count` states (ceil(n/32) words each) against the
+ * caller's W (diagonal included, as compute_cut / compute_energy,
+ * maxcut_tfim_util.py:319-331): cut[b] = 1/2 sum_{u,v} W_uv [s_u != s_v],
+ * energy[b] = 1/2 sum_{u,v} W_uv (2[s_u != s_v] - 1). Either output nullable.
+ * Deterministic (fixed reduction order).
+ */
+pqi_status pqi_rescore_fp64(const pqi_weights* w, const uint32_t* theta, int count, double* cut,
+                            double* energy, void* workspace, size_t workspace_bytes,
+                            void* stream);
+
+/* bools (rows x n bytes, nonzero = 1) -> words (rows x ceil(n/32) uint32).
+ * Replaces convert_bool_to_uint (maxcut_tfim_util.py:304-316). */
+pqi_status pqi_pack_bits(const uint8_t* bools, int rows, int n, uint32_t* words, void* stream);
+
+/* words (rows x ceil(n/32)) -> bytes 0/1 (rows x n). */
+pqi_status pqi_unpack_bits(const uint32_t* words, int rows, int n, uint8_t* bools, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PQI_H */

@@ -1,0 +1,17 @@
+"""B200-native drop-in for PyQrackIsing's dense cut-scoring and local-search path.
+
+Public API (same signatures and return tuples as the reference):
+  maxcut_tfim(G, quality, shots, is_spin_glass, anneal_t, anneal_h,
+              repulsion_base, is_maxcut_gpu, is_nested)
+  spin_glass_solver(G, quality, shots, best_guess, is_maxcut_gpu, is_spin_glass,
+                    anneal_t, anneal_h, repulsion_base, is_log, gray_iterations,
+                    gray_seed_multiple, bp_scale, bp_damping)
+
+All arithmetic on the coupling matrix runs in libpqi.so (hand-written sm_100a
+CUDA behind the C ABI in include/pqi.h); there is no CPU fallback.
+"""
+
+from .maxcut_tfim import maxcut_tfim
+from .spin_glass_solver import spin_glass_solver
+
+__all__ = ["maxcut_tfim", "spin_glass_solver"]

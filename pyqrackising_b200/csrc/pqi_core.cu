@@ -1,0 +1,659 @@
+// libpqi core: set-up, weight preparation, gains, selection, single/double
+// flip passes, flip application, fp64 re-scoring and bit packing (sm_100a).
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "pqi_common.cuh"
+
+namespace pqi {
+
+static thread_local char g_last_error[256] = {0};
+
+void set_error(cudaError_t e, const char* where) {
+  snprintf(g_last_error, sizeof(g_last_error), "%s: %s", where, cudaGetErrorString(e));
+}
+
+bool make_sel_geom(long count, int G, int L, SelGeom* out) {
+  if (G <= 0 || L <= 0 || L > 64 || G % L != 0 || count < 0) return false;
+  long long J = (count + G - 1) / G;
+  if (J < 1) J = 1;
+  if ((unsigned long long)G * (unsigned long long)J >= 0xFFFFFFFFull) return false;
+  out->G = (uint32_t)G;
+  out->L = (uint32_t)L;
+  out->J = (uint32_t)J;
+  memset(out->rank, 0xFF, sizeof(out->rank));
+  memset(out->slot_of_rank, 0, sizeof(out->slot_of_rank));
+  // Replay reduce_energy_index (kernels.cl:8-20) with every unranked slot tied:
+  // slot t < off absorbs t + off only when t holds nothing better, i.e. a tie
+  // keeps t. The slot that reaches 0 is the next in tie order.
+  bool ranked[64] = {false};
+  for (int r = 0; r < L; ++r) {
+    bool present[64];
+    int id[64];
+    for (int t = 0; t < L; ++t) {
+      present[t] = !ranked[t];
+      id[t] = t;
+    }
+    for (int off = L >> 1; off > 0; off >>= 1) {
+      for (int t = 0; t < off; ++t) {
+        if (!present[t] && present[t + off]) {
+          present[t] = true;
+          id[t] = id[t + off];
+        }
+      }
+    }
+    if (!present[0]) break;
+    out->rank[id[0]] = (uint8_t)r;
+    out->slot_of_rank[r] = (uint8_t)id[0];
+    ranked[id[0]] = true;
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Weight preparation
+
+struct PrepStats {
+  unsigned long long nonfinite;
+  unsigned long long nonint;
+  unsigned long long asym;
+  unsigned int maxabs_bits;
+  unsigned int pad;
+};
+
+// One 32x32 tile per block (32 x 8 threads): compares W[i][j] with W[j][i],
+// classifies values and sums the upper triangle in float64.
+__global__ void prep_scan_kernel(const float* __restrict__ W, int n, PrepStats* st,
+                                 double* __restrict__ partial) {
+  __shared__ float tT[32][33];
+  __shared__ double red[256];
+  __shared__ unsigned int red_u[3][256];
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int bi = blockIdx.y, bj = blockIdx.x;
+  // tile (bj, bi): rows bj*32.., cols bi*32..
+  for (int r = ty; r < 32; r += 8) {
+    const int row = bj * 32 + r, col = bi * 32 + tx;
+    tT[r][tx] = (row < n && col < n) ? W[(size_t)row * n + col] : 0.0f;
+  }
+  __syncthreads();
+  double up = 0.0;
+  unsigned int nf = 0, ni = 0, as = 0;
+  float mx = 0.0f;
+  for (int r = ty; r < 32; r += 8) {
+    const int i = bi * 32 + r, j = bj * 32 + tx;
+    if (i < n && j < n) {
+      const float w = W[(size_t)i * n + j];
+      const float wt = tT[tx][r];  // W[j][i]
+      if (!isfinite(w)) {
+        ++nf;
+      } else {
+        if (i != j) {
+          if (w != rintf(w)) ++ni;
+          mx = fmaxf(mx, fabsf(w));
+          if (w != wt) ++as;
+          if (i < j) up += (double)w;
+        }
+      }
+    }
+  }
+  const int tid = ty * 32 + tx;
+  red[tid] = up;
+  red_u[0][tid] = nf;
+  red_u[1][tid] = ni;
+  red_u[2][tid] = as;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (tid < s) {
+      red[tid] += red[tid + s];
+      red_u[0][tid] += red_u[0][tid + s];
+      red_u[1][tid] += red_u[1][tid + s];
+      red_u[2][tid] += red_u[2][tid + s];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    partial[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = red[0];
+    if (red_u[0][0]) atomicAdd(&st->nonfinite, (unsigned long long)red_u[0][0]);
+    if (red_u[1][0]) atomicAdd(&st->nonint, (unsigned long long)red_u[1][0]);
+    if (red_u[2][0]) atomicAdd(&st->asym, (unsigned long long)red_u[2][0]);
+  }
+  // max |w|: non-negative floats order like their bit patterns
+  unsigned int mb = __float_as_uint(mx);
+  for (int o = 16; o > 0; o >>= 1) mb = max(mb, __shfl_xor_sync(0xFFFFFFFFu, mb, o));
+  if (tx == 0 && mb) atomicMax(&st->maxabs_bits, mb);
+}
+
+// Deterministic sum of `count` doubles by one block.
+__global__ void sum_partials_kernel(const double* __restrict__ p, size_t count, double* out) {
+  __shared__ double red[1024];
+  double s = 0.0;
+  for (size_t i = threadIdx.x; i < count; i += blockDim.x) s += p[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = blockDim.x >> 1; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+// Zero-diagonal, zero-padded copies with row pitch ld.
+__global__ void prep_convert_kernel(const float* __restrict__ W, int n, int ld,
+                                    float* __restrict__ Wz, int8_t* __restrict__ Wi8,
+                                    uint16_t* __restrict__ Whi, uint16_t* __restrict__ Wlo) {
+  const size_t total = (size_t)n * ld;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e / ld), j = (int)(e - (size_t)i * ld);
+    const float w = (j < n && i != j) ? W[(size_t)i * n + j] : 0.0f;
+    Wz[e] = w;
+    if (Wi8) Wi8[e] = (int8_t)(int)w;
+    if (Whi) {
+      const __nv_bfloat16 hi = __float2bfloat16_rn(w);
+      const __nv_bfloat16 lo = __float2bfloat16_rn(w - __bfloat162float(hi));
+      Whi[e] = __bfloat16_as_ushort(hi);
+      Wlo[e] = __bfloat16_as_ushort(lo);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gains: g_k = x_k * sum_v W_kv x_v, x = 2s - 1, one warp per row.
+
+__device__ __forceinline__ double dot_bits(const float4& w, uint32_t bits4) {
+  double a = 0.0;
+  a += (bits4 & 1u) ? (double)w.x : -(double)w.x;
+  a += (bits4 & 2u) ? (double)w.y : -(double)w.y;
+  a += (bits4 & 4u) ? (double)w.z : -(double)w.z;
+  a += (bits4 & 8u) ? (double)w.w : -(double)w.w;
+  return a;
+}
+
+__device__ __forceinline__ int dot_bits_i8(const int4& w, uint32_t bits16) {
+  int a = 0;
+  const int32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int v = (int)(int8_t)((ws[q] >> (8 * b)) & 0xFF);
+      a += ((bits16 >> (q * 4 + b)) & 1u) ? v : -v;
+    }
+  }
+  return a;
+}
+
+// grid: (row blocks, count). Rows of the prepared copy have pitch ld.
+template <typename WT>
+__global__ void gains_gemv_kernel(const WT* __restrict__ Wp, int ld, int n,
+                                  const uint32_t* __restrict__ theta, int n32,
+                                  float* __restrict__ g32, double* __restrict__ g64) {
+  const int lane = threadIdx.x & 31;
+  const int warps = blockDim.x >> 5;
+  const uint32_t* th = theta + (size_t)blockIdx.y * n32;
+  for (int k = blockIdx.x * warps + (threadIdx.x >> 5); k < n; k += gridDim.x * warps) {
+    const WT* row = Wp + (size_t)k * ld;
+    double acc = 0.0;
+    if constexpr (sizeof(WT) == 4) {
+      for (int v = lane * 4; v < n; v += 128) {
+        const float4 w = *reinterpret_cast<const float4*>(row + v);
+        const uint32_t b4 = (__ldg(th + (v >> 5)) >> (v & 31)) & 0xFu;
+        acc += dot_bits(w, b4);
+      }
+    } else {
+      int ai = 0;
+      for (int v = lane * 16; v < n; v += 512) {
+        const int4 w = *reinterpret_cast<const int4*>(row + v);
+        const uint32_t b16 = (__ldg(th + (v >> 5)) >> (v & 31)) & 0xFFFFu;
+        ai += dot_bits_i8(w, b16);
+      }
+      acc = (double)ai;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+    if (lane == 0) {
+      const double g = get_bit32(th, k) ? acc : -acc;
+      if (g32) g32[(size_t)blockIdx.y * n + k] = (float)g;
+      if (g64) g64[(size_t)blockIdx.y * n + k] = g;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Selection
+
+__global__ void select_kernel(const float* __restrict__ vals, long long count, float scale,
+                              SelGeom geo, unsigned long long* key) {
+  __shared__ uint64_t scratch[32];
+  uint64_t best = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x) {
+    const uint64_t k = sel_key(vals[i] * scale, (uint64_t)i, geo);
+    best = k > best ? k : best;
+  }
+  best = block_max_u64(best, scratch);
+  if (threadIdx.x == 0 && best) atomicMax(key, (unsigned long long)best);
+}
+
+__global__ void select_finish_kernel(const unsigned long long* key, SelGeom geo, float* best_val,
+                                     int* best_idx) {
+  float v;
+  int64_t i;
+  sel_decode(*key, geo, &v, &i);
+  if (best_val) *best_val = v;
+  if (best_idx) *best_idx = (int)i;
+}
+
+// ---------------------------------------------------------------------------
+// Double flips: one block per row k, threads over l > k.
+
+template <typename WT>
+__global__ void double_kernel(const WT* __restrict__ Wp, int ld, int n,
+                              const uint32_t* __restrict__ theta, const double* __restrict__ g64,
+                              int spin, SelGeom geo, unsigned long long* key) {
+  __shared__ uint64_t scratch[32];
+  uint64_t best = 0;
+  for (int k = blockIdx.x; k < n - 1; k += gridDim.x) {
+    const double gk = g64[k];
+    const int xk = get_bit32(theta, k);
+    const long long base = pair_base(k, n) - (k + 1);
+    const WT* row = Wp + (size_t)k * ld;
+    for (int l = k + 1 + threadIdx.x; l < n; l += blockDim.x) {
+      const double w = (double)row[l];
+      const double d = gk + __ldg(g64 + l) - ((get_bit32(theta, l) == xk) ? 2.0 * w : -2.0 * w);
+      float v = (float)d;
+      if (spin) v *= 2.0f;
+      const uint64_t kk = sel_key(v, (uint64_t)(base + l), geo);
+      best = kk > best ? kk : best;
+    }
+  }
+  best = block_max_u64(best, scratch);
+  if (threadIdx.x == 0 && best) atomicMax(key, (unsigned long long)best);
+}
+
+// ---------------------------------------------------------------------------
+// Apply one or two flips to (theta, gains64). x = 2s - 1 of the state before.
+
+template <typename WT>
+__global__ void apply_flip_gains_kernel(const WT* __restrict__ Wp, int ld, int n,
+                                        const uint32_t* __restrict__ theta,
+                                        double* __restrict__ g64, int k, int l) {
+  const double xk = get_bit32(theta, k) ? 1.0 : -1.0;
+  const double xl = (l >= 0) ? (get_bit32(theta, l) ? 1.0 : -1.0) : 0.0;
+  const WT* rk = Wp + (size_t)k * ld;
+  const WT* rl = (l >= 0) ? Wp + (size_t)l * ld : nullptr;
+  for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const double xv = get_bit32(theta, v) ? 1.0 : -1.0;
+    double g = g64[v];
+    if (l < 0) {
+      g = (v == k) ? -g : g - 2.0 * xv * xk * (double)rk[v];
+    } else if (v == k) {
+      g = -g + 2.0 * xk * xl * (double)rl[k];
+    } else if (v == l) {
+      g = -(g - 2.0 * xl * xk * (double)rk[l]);
+    } else {
+      g = g - 2.0 * xv * xk * (double)rk[v] - 2.0 * xv * xl * (double)rl[v];
+    }
+    g64[v] = g;
+  }
+}
+
+__global__ void toggle_bits_kernel(uint32_t* theta, int k, int l) {
+  theta[k >> 5] ^= 1u << (k & 31);
+  if (l >= 0) theta[l >> 5] ^= 1u << (l & 31);
+}
+
+// ---------------------------------------------------------------------------
+// fp64 re-scoring against the caller's W (diagonal included).
+// grid (row blocks, count); warp per row; partial[b][blk] = (D, T).
+
+__global__ void rescore_kernel(const float* __restrict__ W, int n,
+                               const uint32_t* __restrict__ theta, int n32,
+                               double* __restrict__ partial) {
+  __shared__ double sd[32], stt[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int warps = blockDim.x >> 5;
+  const uint32_t* th = theta + (size_t)blockIdx.y * n32;
+  double d = 0.0, t = 0.0;
+  for (int u = blockIdx.x * warps + warp; u < n; u += gridDim.x * warps) {
+    const float* row = W + (size_t)u * n;
+    const int su = get_bit32(th, u);
+    for (int v = lane; v < n; v += 32) {
+      const double w = (double)row[v];
+      t += w;
+      if (get_bit32(th, v) != su) d += w;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
+    t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
+  }
+  if (lane == 0) {
+    sd[warp] = d;
+    stt[warp] = t;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double D = 0.0, T = 0.0;
+    for (int w = 0; w < warps; ++w) {
+      D += sd[w];
+      T += stt[w];
+    }
+    double* p = partial + ((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 2;
+    p[0] = D;
+    p[1] = T;
+  }
+}
+
+__global__ void rescore_finish_kernel(const double* __restrict__ partial, int nblk, int count,
+                                      double* cut, double* energy) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= count) return;
+  double D = 0.0, T = 0.0;
+  for (int i = 0; i < nblk; ++i) {
+    D += partial[((size_t)b * nblk + i) * 2];
+    T += partial[((size_t)b * nblk + i) * 2 + 1];
+  }
+  if (cut) cut[b] = D / 2.0;
+  if (energy) energy[b] = D - T / 2.0;
+}
+
+// ---------------------------------------------------------------------------
+// Packing
+
+__global__ void pack_kernel(const uint8_t* __restrict__ bools, int rows, int n, int n32,
+                            uint32_t* __restrict__ words) {
+  const long long total = (long long)rows * n32;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e / n32), w = (int)(e - (long long)r * n32);
+    const uint8_t* src = bools + (size_t)r * n + (size_t)w * 32;
+    const int lim = min(32, n - w * 32);
+    uint32_t acc = 0;
+    for (int b = 0; b < lim; ++b) acc |= (src[b] ? 1u : 0u) << b;
+    words[e] = acc;
+  }
+}
+
+__global__ void unpack_kernel(const uint32_t* __restrict__ words, int rows, int n, int n32,
+                              uint8_t* __restrict__ bools) {
+  const long long total = (long long)rows * n;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e / n), j = (int)(e - (long long)r * n);
+    bools[e] = (words[(size_t)r * n32 + (j >> 5)] >> (j & 31)) & 1u;
+  }
+}
+
+static int grid_for(long long work, int block, int cap = 148 * 16) {
+  long long g = (work + block - 1) / block;
+  if (g < 1) g = 1;
+  return (int)std::min<long long>(g, cap);
+}
+
+// Host helpers shared with the other translation units.
+pqi_status launch_gains(const pqi_weights* w, const uint32_t* theta, int count, float* g32,
+                        double* g64, cudaStream_t s) {
+  const int n = w->n, n32 = (n + 31) >> 5;
+  dim3 block(256);
+  dim3 grid((unsigned)std::max(1, std::min((n + 7) / 8, 148 * 4)), (unsigned)count);
+  if (w->kind == PQI_W_I8) {
+    gains_gemv_kernel<int8_t><<<grid, block, 0, s>>>(w->W_i8, w->ld, n, theta, n32, g32, g64);
+  } else {
+    gains_gemv_kernel<float><<<grid, block, 0, s>>>(w->W_f32z, w->ld, n, theta, n32, g32, g64);
+  }
+  PQI_LAUNCHED("gains_gemv_kernel");
+  return PQI_OK;
+}
+
+pqi_status launch_select(const float* vals, long long count, float scale, const SelGeom& geo,
+                         unsigned long long* key, float* best_val, int* best_idx,
+                         cudaStream_t s) {
+  PQI_TRY(cudaMemsetAsync(key, 0, sizeof(unsigned long long), s));
+  select_kernel<<<grid_for(count, 256, 148 * 8), 256, 0, s>>>(vals, count, scale, geo, key);
+  PQI_LAUNCHED("select_kernel");
+  select_finish_kernel<<<1, 1, 0, s>>>(key, geo, best_val, best_idx);
+  PQI_LAUNCHED("select_finish_kernel");
+  return PQI_OK;
+}
+
+}  // namespace pqi
+
+using namespace pqi;
+
+extern "C" {
+
+const char* pqi_version(void) { return "libpqi 0.1 (sm_100a)"; }
+
+const char* pqi_last_error(void) { return g_last_error; }
+
+pqi_status pqi_check_device(int device) {
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) return PQI_ECUDA;
+  if (p.major != 10) return PQI_ENOTSUP;
+  return PQI_OK;
+}
+
+int pqi_padded_ld(int n) { return ((n + 127) / 128) * 128; }
+
+size_t pqi_workspace_bytes(int n, long count) {
+  if (n < 1) n = 1;
+  if (count < 1) count = 1;
+  const size_t ld = (size_t)pqi_padded_ld(n);
+  const size_t cnt_pad = ((size_t)count + 127) / 128 * 128;
+  size_t b = 1 << 16;                                   // scalars, keys, stats
+  b += cnt_pad * ld * 4;                                // expanded +-1 operand (bf16 x2 worst case)
+  b += ((size_t)ld / 64 + 2) * (size_t)count * 8;       // per-tile partial scores
+  b += (size_t)count * 4 + 256;                         // per-candidate energies
+  b += (size_t)n * 8 * 2 + 512;                         // base gains (f64) and f32 copy
+  const size_t tiles = (size_t)((n + 31) / 32) * ((n + 31) / 32);
+  const size_t nblk = (size_t)std::max(1, std::min((n + 7) / 8, 2048));
+  size_t extra = std::max(tiles * 8, (size_t)count * nblk * 16);  // prep / rescore partials
+  if (n > 24576) extra = std::max(extra, (size_t)count * n * 8);  // gray gains in global memory
+  b += extra;
+  return b;
+}
+
+pqi_status pqi_scan_weights(const float* W, int n, void* workspace, size_t workspace_bytes,
+                            pqi_weight_stats* out, void* stream) {
+  PQI_CHECK_ARG(W && out && n > 0);
+  cudaStream_t s = as_stream(stream);
+  Workspace ws(workspace, workspace_bytes);
+  PrepStats* st = ws.take<PrepStats>(1);
+  double* sum = ws.take<double>(1);
+  const int tb = (n + 31) / 32;
+  double* partial = ws.take<double>((size_t)tb * tb);
+  PQI_CHECK_ARG(st && sum && partial);
+  PQI_TRY(cudaMemsetAsync(st, 0, sizeof(PrepStats), s));
+  prep_scan_kernel<<<dim3(tb, tb), dim3(32, 8), 0, s>>>(W, n, st, partial);
+  PQI_LAUNCHED("prep_scan_kernel");
+  sum_partials_kernel<<<1, 1024, 0, s>>>(partial, (size_t)tb * tb, sum);
+  PQI_LAUNCHED("sum_partials_kernel");
+  PrepStats hs;
+  double hsum = 0.0;
+  PQI_TRY(cudaMemcpyAsync(&hs, st, sizeof(hs), cudaMemcpyDeviceToHost, s));
+  PQI_TRY(cudaMemcpyAsync(&hsum, sum, sizeof(hsum), cudaMemcpyDeviceToHost, s));
+  PQI_TRY(cudaStreamSynchronize(s));
+  out->nonfinite = hs.nonfinite;
+  out->nonint = hs.nonint;
+  out->asym = hs.asym;
+  memcpy(&out->maxabs, &hs.maxabs_bits, 4);
+  out->kind = (hs.nonint == 0 && out->maxabs <= 127.0f) ? PQI_W_I8 : PQI_W_F32;
+  out->upper_sum = hsum;
+  if (hs.nonfinite || hs.asym) return PQI_EINVAL;
+  return PQI_OK;
+}
+
+pqi_status pqi_prepare_weights(const float* W, int n, const pqi_weight_stats* stats,
+                               float* W_f32z, int8_t* W_i8, uint16_t* W_hi, uint16_t* W_lo,
+                               pqi_weights* out, void* stream) {
+  PQI_CHECK_ARG(W && W_f32z && out && stats && n > 0);
+  PQI_CHECK_ARG(stats->nonfinite == 0 && stats->asym == 0);
+  const bool as_int8 = stats->kind == PQI_W_I8;
+  if (as_int8) {
+    PQI_CHECK_ARG(W_i8);
+  } else {
+    PQI_CHECK_ARG(W_hi && W_lo);
+  }
+  cudaStream_t s = as_stream(stream);
+  const int ld = pqi_padded_ld(n);
+  prep_convert_kernel<<<grid_for((long long)n * ld, 256, 148 * 16), 256, 0, s>>>(
+      W, n, ld, W_f32z, as_int8 ? W_i8 : nullptr, as_int8 ? nullptr : W_hi,
+      as_int8 ? nullptr : W_lo);
+  PQI_LAUNCHED("prep_convert_kernel");
+  out->W = W;
+  out->W_f32z = W_f32z;
+  out->W_i8 = as_int8 ? W_i8 : nullptr;
+  out->W_hi = as_int8 ? nullptr : W_hi;
+  out->W_lo = as_int8 ? nullptr : W_lo;
+  out->n = n;
+  out->ld = ld;
+  out->kind = as_int8 ? PQI_W_I8 : PQI_W_F32;
+  out->upper_sum = stats->upper_sum;
+  return PQI_OK;
+}
+
+pqi_status pqi_gains(const pqi_weights* w, const uint32_t* theta, int count, float* gains,
+                     double* gains64, void* workspace, size_t workspace_bytes, void* stream) {
+  (void)workspace;
+  (void)workspace_bytes;
+  PQI_CHECK_ARG(w && theta && count > 0 && (gains || gains64));
+  return launch_gains(w, theta, count, gains, gains64, as_stream(stream));
+}
+
+pqi_status pqi_select(const float* values, long count, int global_size, int local_size,
+                      float* best_value, int* best_index, void* workspace,
+                      size_t workspace_bytes, void* stream) {
+  PQI_CHECK_ARG(values && count > 0);
+  SelGeom geo;
+  PQI_CHECK_ARG(make_sel_geom(count, global_size, local_size, &geo));
+  Workspace ws(workspace, workspace_bytes);
+  unsigned long long* key = ws.take<unsigned long long>(1);
+  PQI_CHECK_ARG(key);
+  return launch_select(values, count, 1.0f, geo, key, best_value, best_index, as_stream(stream));
+}
+
+pqi_status pqi_select_host(const float* values_host, long count, int global_size, int local_size,
+                           float* best_value_host, int* best_index_host) {
+  PQI_CHECK_ARG(values_host && count > 0 && best_value_host && best_index_host);
+  SelGeom geo;
+  PQI_CHECK_ARG(make_sel_geom(count, global_size, local_size, &geo));
+  uint64_t best = 0;
+  for (long i = 0; i < count; ++i) {
+    const uint64_t k = sel_key(values_host[i], (uint64_t)i, geo);
+    best = k > best ? k : best;
+  }
+  float v;
+  int64_t idx;
+  sel_decode(best, geo, &v, &idx);
+  *best_value_host = v;
+  *best_index_host = (int)idx;
+  return PQI_OK;
+}
+
+pqi_status pqi_single_bit_flips(const pqi_weights* w, const uint32_t* theta, int is_spin_glass,
+                                int global_size, int local_size, float* best_energy,
+                                int* best_index, void* workspace, size_t workspace_bytes,
+                                void* stream) {
+  PQI_CHECK_ARG(w && theta);
+  SelGeom geo;
+  PQI_CHECK_ARG(make_sel_geom(w->n, global_size, local_size, &geo));
+  Workspace ws(workspace, workspace_bytes);
+  unsigned long long* key = ws.take<unsigned long long>(1);
+  float* g32 = ws.take<float>(w->n);
+  PQI_CHECK_ARG(key && g32);
+  cudaStream_t s = as_stream(stream);
+  pqi_status rc = launch_gains(w, theta, 1, g32, nullptr, s);
+  if (rc) return rc;
+  return launch_select(g32, w->n, is_spin_glass ? 2.0f : 1.0f, geo, key, best_energy, best_index,
+                       s);
+}
+
+pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
+                                const double* gains64, int is_spin_glass, int global_size,
+                                int local_size, float* best_energy, int* best_index,
+                                void* workspace, size_t workspace_bytes, void* stream) {
+  PQI_CHECK_ARG(w && theta && w->n >= 2 && w->n <= 46341);
+  const int n = w->n;
+  const long long combo = (long long)n * (n - 1) / 2;
+  SelGeom geo;
+  PQI_CHECK_ARG(make_sel_geom(combo, global_size, local_size, &geo));
+  Workspace ws(workspace, workspace_bytes);
+  unsigned long long* key = ws.take<unsigned long long>(1);
+  PQI_CHECK_ARG(key);
+  cudaStream_t s = as_stream(stream);
+  if (!gains64) {
+    double* g = ws.take<double>(n);
+    PQI_CHECK_ARG(g);
+    pqi_status rc = launch_gains(w, theta, 1, nullptr, g, s);
+    if (rc) return rc;
+    gains64 = g;
+  }
+  PQI_TRY(cudaMemsetAsync(key, 0, sizeof(unsigned long long), s));
+  const int grid = std::min(n - 1, 148 * 16);
+  if (w->kind == PQI_W_I8) {
+    double_kernel<int8_t><<<grid, 256, 0, s>>>(w->W_i8, w->ld, n, theta, gains64,
+                                               is_spin_glass, geo, key);
+  } else {
+    double_kernel<float><<<grid, 256, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64,
+                                              is_spin_glass, geo, key);
+  }
+  PQI_LAUNCHED("double_kernel");
+  select_finish_kernel<<<1, 1, 0, s>>>(key, geo, best_energy, best_index);
+  PQI_LAUNCHED("select_finish_kernel");
+  return PQI_OK;
+}
+
+pqi_status pqi_apply_flip(const pqi_weights* w, uint32_t* theta, double* gains64, int k, int l,
+                          void* stream) {
+  PQI_CHECK_ARG(w && theta && gains64 && k >= 0 && k < w->n && l < w->n && l != k);
+  cudaStream_t s = as_stream(stream);
+  const int grid = grid_for(w->n, 256, 148 * 4);
+  if (w->kind == PQI_W_I8) {
+    apply_flip_gains_kernel<int8_t><<<grid, 256, 0, s>>>(w->W_i8, w->ld, w->n, theta, gains64, k, l);
+  } else {
+    apply_flip_gains_kernel<float><<<grid, 256, 0, s>>>(w->W_f32z, w->ld, w->n, theta, gains64, k, l);
+  }
+  PQI_LAUNCHED("apply_flip_gains_kernel");
+  toggle_bits_kernel<<<1, 1, 0, s>>>(theta, k, l);
+  PQI_LAUNCHED("toggle_bits_kernel");
+  return PQI_OK;
+}
+
+pqi_status pqi_rescore_fp64(const pqi_weights* w, const uint32_t* theta, int count, double* cut,
+                            double* energy, void* workspace, size_t workspace_bytes,
+                            void* stream) {
+  PQI_CHECK_ARG(w && theta && count > 0 && (cut || energy));
+  const int n = w->n, n32 = (n + 31) >> 5;
+  const int nblk = std::max(1, std::min((n + 7) / 8, 2048));
+  Workspace ws(workspace, workspace_bytes);
+  double* partial = ws.take<double>((size_t)count * nblk * 2);
+  PQI_CHECK_ARG(partial);
+  cudaStream_t s = as_stream(stream);
+  rescore_kernel<<<dim3(nblk, count), 256, 0, s>>>(w->W, n, theta, n32, partial);
+  PQI_LAUNCHED("rescore_kernel");
+  rescore_finish_kernel<<<(count + 127) / 128, 128, 0, s>>>(partial, nblk, count, cut, energy);
+  PQI_LAUNCHED("rescore_finish_kernel");
+  return PQI_OK;
+}
+
+pqi_status pqi_pack_bits(const uint8_t* bools, int rows, int n, uint32_t* words, void* stream) {
+  PQI_CHECK_ARG(bools && words && rows > 0 && n > 0);
+  const int n32 = (n + 31) >> 5;
+  pack_kernel<<<grid_for((long long)rows * n32, 256), 256, 0, as_stream(stream)>>>(bools, rows, n,
+                                                                                n32, words);
+  PQI_LAUNCHED("pack_kernel");
+  return PQI_OK;
+}
+
+pqi_status pqi_unpack_bits(const uint32_t* words, int rows, int n, uint8_t* bools, void* stream) {
+  PQI_CHECK_ARG(bools && words && rows > 0 && n > 0);
+  const int n32 = (n + 31) >> 5;
+  unpack_kernel<<<grid_for((long long)rows * n, 256), 256, 0, as_stream(stream)>>>(words, rows, n,
+                                                                                  n32, bools);
+  PQI_LAUNCHED("unpack_kernel");
+  return PQI_OK;
+}
+
+}  // extern "C"

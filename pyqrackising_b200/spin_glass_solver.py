@@ -1,0 +1,218 @@
+"""Drop-in ``spin_glass_solver`` on the B200 path.
+
+Same signature, defaults and return tuple as the reference
+(``pyqrackising/spin_glass_solver.py:424-727``). The local search follows the
+reference's GPU branch move for move:
+
+1. single-bit-flip passes until none improves (``:608-627``),
+2. then one double-bit-flip pass (``:629-648``), back to 1 if it improved,
+3. then one parallel Gray-code search (``:650-668``), back to 1 if it improved,
+4. else stop (the post-reheat phase, ``:670-717``, re-runs passes 1 and 2 on
+   the unchanged state on this branch, so it cannot improve and is skipped).
+
+Every selection uses the reference's launch geometry, so ties pick the same
+node (``include/pqi.h``). Differences, all deliberate:
+
+* The gains stay on the device and are updated in O(n) per accepted flip; the
+  whole run of single flips is one kernel launch (``pqi_single_descent``)
+  instead of one host round trip per flip.
+* ``gray_seed_multiple`` sets the number of parallel Gray seeds on the GPU (the
+  reference's GPU branch ignores it and uses MAX_GPU_PROC_ELEM, which is the
+  default here too).
+* Returned cut and energy are float64 re-scorings of the returned bit string.
+  The reference returns its running total for one of them (``:720-725``),
+  which drifts after an accepted Gray move (the gray kernel reports half the
+  change, ``kernels.cl:974-976``).
+* ``is_maxcut_gpu`` is accepted and ignored: there is no CPU path.
+* ``bp_scale`` (belief-propagation warm start) is not implemented and raises.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import device as D
+from .maxcut_tfim import maxcut_tfim
+from .util import HEURISTIC_THRESHOLD, as_matrix, get_cut, parse_best_guess
+
+
+def pair_decode(c: int, n: int):
+    """Linear pair index -> (k, l), the reference's enumeration
+    (spin_glass_solver.py:224-234)."""
+    i = 0
+    lcv = n - 1
+    while c >= lcv:
+        c -= lcv
+        i += 1
+        lcv -= 1
+        if not lcv:
+            break
+    return i, c + i + 1
+
+
+class SearchStats:
+    """Counters of one solver run (moves accepted per kind, device flips)."""
+
+    def __init__(self):
+        self.single = 0
+        self.double = 0
+        self.gray = 0
+        self.rounds = 0
+        self.trace = []
+
+    def as_dict(self):
+        return {"single": self.single, "double": self.double, "gray": self.gray, "rounds": self.rounds}
+
+
+def local_search(dg: D.DeviceGraph, theta, is_spin_glass: bool, gray_iterations: int, gray_seeds: int,
+                 mpe: int, max_energy: float, stats: SearchStats | None = None, record_trace: bool = False,
+                 max_rounds: int | None = None):
+    """Run the reference's GPU-branch loop from bool[n] `theta` on a prepared
+    graph. Returns (device words of the final state, running max_energy)."""
+    n = dg.n
+    words = dg.pack(theta)
+    _, g64 = dg.gains(words)
+    Gf, Lf = D.geometry(min(D.WORK_GROUP_MULTIPLE, n), n, mpe)
+    iters_bound = (gray_iterations + gray_seeds - 1) // gray_seeds
+    budget = max(4 * n, 1024)
+    trace = torch.empty(budget, dtype=torch.int32, device=dg.device) if record_trace else None
+    spin = bool(is_spin_glass)
+    rounds = 0
+    while True:
+        rounds += 1
+        if max_rounds is not None and rounds > max_rounds:
+            break
+        # 1. single flips, all on the device
+        while True:
+            esum, flips, rc = dg.single_descent(words, g64, spin, Gf, Lf, budget, trace)
+            nf = int(flips.item())
+            max_energy += float(esum.item())
+            if stats is not None:
+                stats.single += nf
+                if record_trace and nf:
+                    stats.trace.extend(("single", int(k)) for k in trace[:nf].tolist())
+            if rc != 3:  # PQI_ETIMEOUT: budget used up, keep going
+                break
+        # 2. double flips
+        if n >= 2:
+            be, bi = dg.double_bit_flips(words, g64, spin, Gf, Lf)
+            e = float(be.item())
+            if e > 0.0:
+                k, l = pair_decode(int(bi.item()), n)
+                dg.apply_flip(words, g64, k, l)
+                max_energy += e
+                if stats is not None:
+                    stats.double += 1
+                    if record_trace:
+                        stats.trace.append(("double", k, l))
+                continue
+        # 3. parallel Gray-code search
+        tout, eout = dg.gray(words, g64, spin, iters_bound, gray_seeds)
+        be, bi = dg.select(eout, gray_seeds, 1)
+        e = float(be.item())
+        if e > 0.0:
+            bx = int(bi.item())
+            row = tout[bx * 2 * dg.n64 : bx * 2 * dg.n64 + dg.n32].clone()
+            if n & 31:
+                row[-1] &= (1 << (n & 31)) - 1  # bits >= n are padding (the reference unpacks bits < n)
+            words[: dg.n32] = row
+            _, g64 = dg.gains(words)
+            max_energy += e
+            if stats is not None:
+                stats.gray += 1
+                if record_trace:
+                    stats.trace.append(("gray", bx))
+            continue
+        break
+    if stats is not None:
+        stats.rounds = rounds
+    return words, max_energy
+
+
+def spin_glass_solver(
+    G,
+    quality=None,
+    shots=None,
+    best_guess=None,
+    is_maxcut_gpu=True,
+    is_spin_glass=True,
+    anneal_t=None,
+    anneal_h=None,
+    repulsion_base=None,
+    is_log=False,
+    gray_iterations=None,
+    gray_seed_multiple=None,
+    bp_scale=None,
+    bp_damping=0.5,
+):
+    nodes, G_m = as_matrix(G)
+    n_qubits = len(nodes)
+
+    if n_qubits < 3:
+        if n_qubits == 0:
+            return "", 0, ([], []), 0
+        if n_qubits == 1:
+            return "0", 0, (nodes, []), 0
+        if n_qubits == 2:
+            weight = G_m[0, 1]
+            if weight < 0.0:
+                return "00", 0, (nodes, []), weight
+            return "01", weight, ([nodes[0]], [nodes[1]]), -weight
+
+    if n_qubits < HEURISTIC_THRESHOLD:
+        best_guess = None
+
+    theta = parse_best_guess(best_guess, n_qubits)
+    cut_value = None
+    if theta is None:
+        if bp_scale is not None and n_qubits >= HEURISTIC_THRESHOLD:
+            raise NotImplementedError("belief-propagation warm start (bp_scale) is not implemented on this path")
+        bitstring, cut_value, _ = maxcut_tfim(
+            G_m,
+            quality=quality,
+            shots=shots,
+            is_spin_glass=is_spin_glass,
+            anneal_t=anneal_t,
+            anneal_h=anneal_h,
+            repulsion_base=repulsion_base,
+            is_maxcut_gpu=is_maxcut_gpu,
+            is_nested=True,
+        )
+        theta = np.array([b == "1" for b in bitstring], dtype=np.bool_)
+
+    dg = D.DeviceGraph(G_m)
+    words = dg.pack(theta)
+    cut0, en0 = dg.rescore(words)
+    if is_spin_glass:
+        max_energy = float(en0.item())
+    elif cut_value is None:
+        max_energy = float(cut0.item())
+    else:
+        max_energy = cut_value
+
+    if n_qubits < HEURISTIC_THRESHOLD:
+        bitstring, l, r = get_cut(theta, nodes)
+        if is_spin_glass:
+            cut_value = float(cut0.item())
+            min_energy = -max_energy
+        else:
+            cut_value = max_energy
+            min_energy = float(en0.item())
+        return bitstring, float(cut_value), (l, r), float(min_energy)
+
+    if gray_iterations is None:
+        gray_iterations = n_qubits * n_qubits
+    mpe = D.max_gpu_proc_elem(dg.device)
+    seeds = int(gray_seed_multiple) if gray_seed_multiple is not None else mpe
+
+    words, max_energy = local_search(dg, theta, is_spin_glass, int(gray_iterations), seeds, mpe, max_energy)
+
+    best = dg.unpack(words)[0]
+    cut, en = dg.rescore(words)
+    bitstring, l, r = get_cut(best, nodes)
+    cut_value = float(cut.item())
+    min_energy = -float(en.item()) if is_spin_glass else float(en.item())
+    return bitstring, cut_value, (l, r), min_energy

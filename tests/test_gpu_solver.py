@@ -1,0 +1,57 @@
+"""End-to-end parity of the drop-in solver on the GPU against the reference's
+GPU-branch run (golden: the restated driver on the reference's kernels.cl)
+from the same best_guess fixture, and against the reference's CPU solver."""
+
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+
+pytestmark = pytest.mark.gpu
+
+NAMES = golden_names()
+
+
+def _is_int(W):
+    return bool(np.all(W == np.rint(W)) and np.abs(W).max() <= 127)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_spin_glass_solver_matches_reference_gpu_branch(name, monkeypatch, oracle_mod):
+    from pyqrackising_b200 import spin_glass_solver
+
+    monkeypatch.setenv("PYQRACKISING_MAX_GPU_PROC_ELEM", "148")
+    O = oracle_mod
+    d = load_golden(name)
+    W, spin = d["W"], bool(d["is_spin_glass"])
+    bg = [bool(b) for b in d["best_guess"]]
+    bs, cut, (l, r), energy = spin_glass_solver(
+        W, best_guess=bg, is_spin_glass=spin, gray_iterations=int(d["e2e_gray_iterations"])
+    )
+    bits = np.array([c == "1" for c in bs], dtype=bool)
+    assert len(l) + len(r) == W.shape[0]
+    # returned values are the float64 re-scoring of the returned bit string
+    assert cut == pytest.approx(O.compute_cut(bits, W), rel=1e-12, abs=1e-9)
+    e_ref = O.compute_energy(bits, W)
+    assert energy == pytest.approx(-e_ref if spin else e_ref, rel=1e-12, abs=1e-9)
+    if _is_int(W):
+        assert np.array_equal(bits, d["e2e_theta"])
+    else:
+        # float weights: same local search, float rounding may reorder near-ties
+        target = float(d["e2e_energy"] if spin else d["e2e_cut"])
+        got = O.compute_energy(bits, W) if spin else O.compute_cut(bits, W)
+        assert got >= target - 1e-5 * abs(target) or np.array_equal(bits, d["e2e_theta"])
+
+
+def test_small_n_paths():
+    from pyqrackising_b200 import maxcut_tfim, spin_glass_solver
+
+    d = load_golden("exact")
+    W = d["W_12"]
+    bs, v, (l, r) = maxcut_tfim(W)
+    assert v == float(d["maxcut_value_12"])
+    assert bs == "".join("1" if b else "0" for b in d["maxcut_bits_12"])
+    assert spin_glass_solver(np.zeros((0, 0), np.float32)) == ("", 0, ([], []), 0)
+    assert spin_glass_solver(np.zeros((1, 1), np.float32))[0] == "0"
+    W2 = np.array([[0, 2.5], [2.5, 0]], np.float32)
+    assert spin_glass_solver(W2)[:2] == ("01", np.float32(2.5))

@@ -1,0 +1,42 @@
+"""Host-side logic of the drop-in (no GPU): launch geometry, pair decoding,
+best_guess parsing, result formatting."""
+
+import importlib
+
+import numpy as np
+
+from pyqrackising_b200 import device as D
+from pyqrackising_b200 import util
+
+S = importlib.import_module("pyqrackising_b200.spin_glass_solver")
+
+
+def test_geometry_matches_setup_opencl(oracle_mod):
+    for n in (3, 24, 31, 64, 100, 2048, 8192):
+        for mpe in (1, 7, 148, 4096):
+            assert D.geometry(min(32, n), n, mpe) == oracle_mod.flip_geometry(n, mpe)
+    assert D.geometry(1, 148, 148) == (148, 1)
+    assert D.geometry(2048, 2048, 148) == (160, 32)
+
+
+def test_pair_decode_matches_reference_loop(oracle_mod):
+    for n in (2, 3, 10, 57):
+        c = 0
+        for k in range(n):
+            for l in range(k + 1, n):
+                assert S.pair_decode(c, n) == (k, l) == oracle_mod.pair_decode(c, n)
+                c += 1
+
+
+def test_best_guess_parsing():
+    n = 8
+    assert util.parse_best_guess("10110000", n).tolist() == [True, False, True, True, False, False, False, False]
+    assert util.parse_best_guess(13, n).tolist() == [True, False, True, True, False, False, False, False]
+    assert util.parse_best_guess([1, 0, 1], 3).tolist() == [True, False, True]
+    assert util.parse_best_guess(None, n) is None
+    assert util.parse_best_guess(np.int64(3), n) is None  # the reference only accepts a Python int
+
+
+def test_get_cut():
+    bs, l, r = util.get_cut(np.array([1, 0, 1], bool), ["a", "b", "c"])
+    assert bs == "101" and l == ["b"] and r == ["a", "c"]
