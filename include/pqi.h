@@ -176,6 +176,29 @@ pqi_status pqi_single_bit_flips(const pqi_weights* w, const uint32_t* theta, int
                                 int* best_index, void* workspace, size_t workspace_bytes,
                                 void* stream);
 
+/* Largest n pqi_single_bit_flips_noalloc accepts, and the bytes of the device
+ * array it uses in place of a workspace (a selection key, then n floats). */
+#define PQI_NOALLOC_MAX_N 65536
+#define PQI_NOALLOC_BYTES (256 + 4 * PQI_NOALLOC_MAX_N)
+
+/*
+ * pqi_single_bit_flips without a workspace, for callers that cannot allocate
+ * device memory: a process whose device memory belongs to another framework's
+ * allocator, or a loop that must not call cudaMalloc because it can synchronise
+ * the device. No counterpart in the reference (its OpenCL host glue allocates
+ * buffers on every call, maxcut_tfim_util.py:169-221).
+ * Scratch is one array of PQI_NOALLOC_BYTES compiled into the library, held by
+ * every GPU that loads it until exit. The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress, with the device current); make
+ * it before any stream capture. All calls share the array, which keeps the last
+ * call's contents: calls that overlap on the GPU race. Allocates nothing.
+ * Returns PQI_EINVAL when n > PQI_NOALLOC_MAX_N (pqi_last_error() says so).
+ * Same outputs as pqi_single_bit_flips.
+ */
+pqi_status pqi_single_bit_flips_noalloc(const pqi_weights* w, const uint32_t* theta,
+                                        int is_spin_glass, int global_size, int local_size,
+                                        float* best_energy, int* best_index, void* stream);
+
 /*
  * One double-bit-flip pass over all pairs k < l in the reference's linear
  * order c = k(n-1) - k(k-1)/2 + (l-k-1) (kernels.cl:206-218): value_c =

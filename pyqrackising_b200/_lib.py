@@ -23,6 +23,8 @@ _NAMES = {1: "PQI_EINVAL", 2: "PQI_ECUDA", 3: "PQI_ETIMEOUT", 4: "PQI_ENOTSUP"}
 PQI_W_F32 = 0
 PQI_W_I8 = 1
 
+PQI_NOALLOC_MAX_N = 65536  # include/pqi.h
+
 
 class PQIUnavailable(ImportError):
     pass
@@ -84,6 +86,7 @@ SIGNATURES = {
     "pqi_select": (_i, [_vp, _l, _i, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_select_host": (_i, [_vp, _l, _i, _i, _vp, _vp]),
     "pqi_single_bit_flips": (_i, [_WP, _vp, _i, _i, _i, _vp, _vp, _vp, _sz, _vp]),
+    "pqi_single_bit_flips_noalloc": (_i, [_WP, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "pqi_double_bit_flips": (_i, [_WP, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_gray": (_i, [_WP, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_single_descent": (_i, [_WP, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _sz, _vp]),

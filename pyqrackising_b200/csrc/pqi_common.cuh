@@ -14,6 +14,7 @@ namespace pqi {
 
 // Last CUDA error seen by the library (host side, for diagnostics).
 void set_error(cudaError_t e, const char* where);
+void set_error_text(const char* msg);
 
 #define PQI_TRY(expr)                                  \
   do {                                                 \

@@ -15,6 +15,8 @@ void set_error(cudaError_t e, const char* where) {
   snprintf(g_last_error, sizeof(g_last_error), "%s: %s", where, cudaGetErrorString(e));
 }
 
+void set_error_text(const char* msg) { snprintf(g_last_error, sizeof(g_last_error), "%s", msg); }
+
 bool make_sel_geom(long count, int G, int L, SelGeom* out) {
   if (G <= 0 || L <= 0 || L > 64 || G % L != 0 || count < 0) return false;
   long long J = (count + G - 1) / G;
