@@ -121,6 +121,11 @@ pqi_status pqi_prepare_weights(const float* W, int n, const pqi_weight_stats* st
  * default), 1 = CUDA cores. Process-wide; used to cross-check the two. */
 pqi_status pqi_score_set_path(int path);
 
+/* Record two caller-owned cudaEvent_t on the call's stream immediately before
+ * and after the scoring GEMM launch inside each later pqi_calculate_cut (NULL,
+ * NULL to stop). Process-wide; lets a caller time the GEMM kernel alone. */
+pqi_status pqi_score_set_events(void* before, void* after);
+
 /* ---------------------------------------------------------------------------
  * Kernel-level replacements of the reference's OpenCL kernels
  * -------------------------------------------------------------------------*/
@@ -133,7 +138,8 @@ pqi_status pqi_score_set_path(int path);
  * geometry (G, L) to best_energy/best_index (device scalars). Integer
  * weights run on the int8 tensor-core path with int32 accumulation (exact);
  * float weights on the split-bf16 tensor-core path with fp32 accumulation.
- * Replaces calculate_cut (kernels.cl:64-94) plus the host argmax of
+ * If the tensor-core kernel gives up (a bounded wait expired), energies are
+ * NaN and best_index is -1. Replaces calculate_cut (kernels.cl:64-94) plus the host argmax of
  * run_cut_opencl (maxcut_tfim.py:212-285).
  */
 pqi_status pqi_calculate_cut(const pqi_weights* w, const uint32_t* theta, int shots,

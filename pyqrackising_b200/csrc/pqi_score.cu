@@ -8,7 +8,8 @@
 // where S = sum_{u<v} W_uv. q is the row-dot of X with Y = X W, so the batch is
 // one GEMM plus an epilogue. This file holds the CUDA-core tiled path; the
 // tensor-core (tcgen05) path lives in pqi_score_tc.cu and shares the finish
-// kernel below.
+// kernel below. A failed tensor-core launch (a bounded wait that expired)
+// surfaces as NaN values and best_index -1.
 #include <algorithm>
 
 #include "pqi_common.cuh"
@@ -88,14 +89,16 @@ __global__ void __launch_bounds__(256) xw_rowdot_kernel(const WT* __restrict__ W
 // value, store it and fold it into the selection key.
 __global__ void score_finish_kernel(const double* __restrict__ qpart, int tiles, int shots,
                                     double upper_sum, int spin, SelGeom geo,
-                                    float* __restrict__ energies, unsigned long long* key) {
+                                    float* __restrict__ energies, unsigned long long* key,
+                                    const int* __restrict__ err) {
   __shared__ uint64_t scratch[32];
   uint64_t best = 0;
+  const bool failed = err && *err;
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < shots; b += gridDim.x * blockDim.x) {
     double q = 0.0;
     for (int t = 0; t < tiles; ++t) q += qpart[(size_t)t * shots + b];
     const double val = spin ? -q / 2.0 : (2.0 * upper_sum - q) / 4.0;
-    const float v = (float)val;
+    const float v = failed ? __int_as_float(0x7FC00000) : (float)val;  // NaN marks a failed GEMM
     if (energies) energies[b] = v;
     const uint64_t k = sel_key(v, (uint64_t)b, geo);
     best = k > best ? k : best;
@@ -105,23 +108,28 @@ __global__ void score_finish_kernel(const double* __restrict__ qpart, int tiles,
 }
 
 __global__ void score_select_finish_kernel(const unsigned long long* key, SelGeom geo,
-                                           float* best_val, int* best_idx) {
+                                           float* best_val, int* best_idx,
+                                           const int* __restrict__ err) {
   float v;
   int64_t i;
   sel_decode(*key, geo, &v, &i);
+  if (err && *err) {
+    v = __int_as_float(0x7FC00000);
+    i = -1;
+  }
   if (best_val) *best_val = v;
   if (best_idx) *best_idx = (int)i;
 }
 
 pqi_status score_finish(const double* qpart, int tiles, int shots, double upper_sum, int spin,
                         const SelGeom& geo, float* energies, unsigned long long* key,
-                        float* best_energy, int* best_index, cudaStream_t s) {
+                        float* best_energy, int* best_index, const int* err, cudaStream_t s) {
   PQI_TRY(cudaMemsetAsync(key, 0, sizeof(unsigned long long), s));
   const int grid = std::max(1, std::min((shots + 255) / 256, 148 * 4));
   score_finish_kernel<<<grid, 256, 0, s>>>(qpart, tiles, shots, upper_sum, spin, geo, energies,
-                                           key);
+                                           key, err);
   PQI_LAUNCHED("score_finish_kernel");
-  score_select_finish_kernel<<<1, 1, 0, s>>>(key, geo, best_energy, best_index);
+  score_select_finish_kernel<<<1, 1, 0, s>>>(key, geo, best_energy, best_index, err);
   PQI_LAUNCHED("score_select_finish_kernel");
   return PQI_OK;
 }
@@ -144,8 +152,12 @@ pqi_status score_simt(const pqi_weights* w, const uint32_t* theta, int shots, do
 // 1 = CUDA cores only. Used by tests to compare the two paths.
 int g_score_path = 0;
 
-pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, double* qpart,
-                    int* tiles_out, Workspace& ws, cudaStream_t s);
+pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int spin,
+                    const SelGeom& geo, float* energies, float* best_energy, int* best_index,
+                    Workspace& ws, cudaStream_t s);
+
+// Optional events recorded around the scoring GEMM launch (bench timing).
+cudaEvent_t g_score_ev_before = nullptr, g_score_ev_after = nullptr;
 
 }  // namespace pqi
 
@@ -156,6 +168,12 @@ extern "C" {
 pqi_status pqi_score_set_path(int path) {
   if (path < 0 || path > 1) return PQI_EINVAL;
   g_score_path = path;
+  return PQI_OK;
+}
+
+pqi_status pqi_score_set_events(void* before, void* after) {
+  g_score_ev_before = reinterpret_cast<cudaEvent_t>(before);
+  g_score_ev_after = reinterpret_cast<cudaEvent_t>(after);
   return PQI_OK;
 }
 
@@ -170,30 +188,21 @@ pqi_status pqi_calculate_cut(const pqi_weights* w, const uint32_t* theta, int sh
   Workspace ws(workspace, workspace_bytes);
   unsigned long long* key = ws.take<unsigned long long>(1);
   PQI_CHECK_ARG(key);
-  int tiles = 0;
-  double* qpart = nullptr;
-  pqi_status rc = PQI_ENOTSUP;
   if (g_score_path == 0) {
-    Workspace ws_try = ws;
-    rc = score_tc(w, theta, shots, nullptr, &tiles, ws_try, s);  // query tile count
-    if (rc == PQI_OK) {
-      qpart = ws_try.take<double>((size_t)tiles * shots);
-      PQI_CHECK_ARG(qpart);
-      rc = score_tc(w, theta, shots, qpart, &tiles, ws_try, s);
-      if (rc != PQI_OK) return rc;
-    }
+    pqi_status rc = score_tc(w, theta, shots, is_spin_glass, geo, energies, best_energy,
+                             best_index, ws, s);
+    if (rc != PQI_ENOTSUP) return rc;
   }
-  if (rc == PQI_ENOTSUP) {
-    tiles = (w->n + kBN - 1) / kBN;
-    qpart = ws.take<double>((size_t)tiles * shots);
-    PQI_CHECK_ARG(qpart);
-    rc = score_simt(w, theta, shots, qpart, s);
-    if (rc != PQI_OK) return rc;
-  } else if (rc != PQI_OK) {
-    return rc;
-  }
+  const int tiles = (w->n + kBN - 1) / kBN;
+  double* qpart = ws.take<double>((size_t)tiles * shots);
+  PQI_CHECK_ARG(qpart);
+  if (g_score_ev_before) PQI_TRY(cudaEventRecord(g_score_ev_before, s));
+  pqi_status rc = score_simt(w, theta, shots, qpart, s);
+  if (g_score_ev_after) PQI_TRY(cudaEventRecord(g_score_ev_after, s));
+  if (rc != PQI_OK) return rc;
+  const int* err = nullptr;
   return score_finish(qpart, tiles, shots, w->upper_sum, is_spin_glass, geo, energies, key,
-                      best_energy, best_index, s);
+                      best_energy, best_index, err, s);
 }
 
 }  // extern "C"

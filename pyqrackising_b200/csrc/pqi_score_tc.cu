@@ -1,9 +1,571 @@
-// placeholder, replaced by the tcgen05 path
+// libpqi: tensor-core (tcgen05) batched scoring for sm_100a.
+//
+// Y = X W for a batch of candidates X (B x n, entries +-1) and the coupling
+// matrix W (n x n, symmetric, zero diagonal), then q_b = sum_j x_bj Y_bj in the
+// epilogue (score_finish in pqi_score.cu turns q into the reference's value).
+//
+//  * int8 path (integer weights in [-127, 127]): A = X as int8 +-1, B = W_i8,
+//    kind::i8 MMAs with int32 accumulation: exact.
+//  * float path: W = hi + lo (two bf16 matrices), A = X as bf16 +-1, two K
+//    passes (hi then lo) into one float32 accumulator (kind::f16).
+//
+// A persistent CTA per SM walks 128 x 256 tiles of Y (candidates x nodes),
+// each over all of K, with a 4-stage shared-memory ring and two 256-column
+// TMEM accumulators so the epilogue of one tile overlaps the MMAs of the next:
+//   warp 0    : TMA loads of the +-1 candidate tile (expanded from the packed
+//               bits by a short pass, L2-resident) and of the W tile (W is
+//               symmetric, so its rows are the K-major rows the B operand
+//               needs); ragged edges come from the TMA zero fill
+//   warp 1    : TMEM allocation; lane 0 issues tcgen05.mma
+//   warps 2-5 : epilogue: tcgen05.ld, row-dot with x, one partial per row;
+//               the last tile of a candidate block folds the block into the
+//               reference-order selection (no separate finish launch)
+// Every mbarrier wait is bounded by a clock budget; on expiry the CTA records
+// an error, the outputs become NaN / index -1, and TMEM is still released.
+#include <cuda.h>
+
+#include <algorithm>
+
 #include "pqi_common.cuh"
+
 namespace pqi {
-pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, double* qpart,
-                    int* tiles_out, Workspace& ws, cudaStream_t s) {
-  (void)w; (void)theta; (void)shots; (void)qpart; (void)tiles_out; (void)ws; (void)s;
-  return PQI_ENOTSUP;
+
+namespace tc {
+
+constexpr int BM = 128;           // candidates per tile (UMMA M)
+constexpr int BN = 256;           // nodes per tile (UMMA N)
+constexpr int BK_BYTES = 128;     // K bytes per stage (one 128-byte swizzle row)
+constexpr int STAGES = 4;
+constexpr int A_STAGE = BM * BK_BYTES;   // 16 KB
+constexpr int B_STAGE = BN * BK_BYTES;   // 32 KB
+constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+constexpr long long WAIT_BUDGET_CYCLES = 4000000000ll;  // ~2 s at 1.9 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// Bounded wait for the phase with parity `parity`; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  const long long t0 = clock64();
+  while (true) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > WAIT_BUDGET_CYCLES) return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x,
+                                            int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+      "%4}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
+
+// K-major operand tile with 128-byte swizzle: 8-row groups 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);  // start address (16-byte units)
+  d |= (uint64_t)1 << 16;                   // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset: 8 rows x 128 B
+  d |= (uint64_t)1 << 46;                   // descriptor version for sm_100
+  d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
+  return d;
+}
+
+template <bool kInt8>
+__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                    uint32_t accumulate) {
+  if constexpr (kInt8) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+  } else {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+  }
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_load32_nowait(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Instruction descriptors (M = 128, N = 256, both operands K-major).
+constexpr uint32_t kIdescI8 = (2u << 4)      // D: s32
+                              | (1u << 7)    // A: signed int8
+                              | (1u << 10)   // B: signed int8
+                              | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+constexpr uint32_t kIdescBF16 = (1u << 4)    // D: f32
+                                | (1u << 7)  // A: bf16
+                                | (1u << 10) // B: bf16
+                                | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+// Warp roles of the persistent kernel (6 warps).
+constexpr int TMA_WARP = 0;       // warp 0 lane 0: TMA loads of the X and W tiles
+constexpr int MMA_WARP = 1;       // warp 1: TMEM alloc, lane 0 issues MMAs
+constexpr int PTHREADS = 192;     // warps 2-5: epilogue (TMEM lane quarter = warp % 4)
+constexpr int ACC_COLS = 512;     // two 256-column accumulators
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+
+// Persistent scoring kernel: CTA c handles tiles c, c + gridDim.x, ...; tile t
+// covers candidates [128 * (t / ntn), +128) x nodes [256 * (t % ntn), +256).
+// The last CTA to finish a candidate block sums that block's node-tile
+// partials in a fixed order, converts q to the reference's value and folds it
+// into the selection key; the last candidate block decodes the selection.
+template <bool kInt8>
+__global__ void __launch_bounds__(PTHREADS, 1)
+    score_tc_kernel(const __grid_constant__ CUtensorMap map_a,
+                    const __grid_constant__ CUtensorMap map_b0,
+                    const __grid_constant__ CUtensorMap map_b1, int n, int shots,
+                    const uint32_t* __restrict__ theta, int n32, double upper_sum, int spin,
+                    SelGeom geo, double* __restrict__ qpart, float* __restrict__ energies,
+                    unsigned int* __restrict__ mcount, unsigned int* __restrict__ mdone,
+                    unsigned long long* __restrict__ key, float* __restrict__ best_energy,
+                    int* __restrict__ best_index, int* __restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[STAGES];
+  __shared__ __align__(8) uint64_t accf_bar[2];
+  __shared__ __align__(8) uint64_t acce_bar[2];
+  __shared__ uint32_t tmem_base_holder;
+  __shared__ int s_fail;
+  __shared__ unsigned int s_bcast;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t raw = smem_u32(smem_raw);
+  uint8_t* smem = smem_raw + ((1024 - (raw & 1023)) & 1023);
+
+  const int ntn = (n + BN - 1) / BN;
+  const int ntm = (shots + BM - 1) / BM;
+  const int ntiles = ntn * ntm;
+  const int kb_per_pass = kInt8 ? (n + BK_BYTES - 1) / BK_BYTES : (n + 63) / 64;
+  const int kblocks = kInt8 ? kb_per_pass : 2 * kb_per_pass;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full_bar[s], 1);
+      mbar_init(&empty_bar[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&accf_bar[a], 1);
+      mbar_init(&acce_bar[a], 4);
+    }
+    s_fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == MMA_WARP) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&tmem_base_holder)),
+                 "r"(ACC_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem_base = tmem_base_holder;
+
+  if (warp == TMA_WARP) {
+    if (lane == 0) {
+      uint32_t it = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
+        for (int kb = 0; kb < kblocks; ++kb, ++it) {
+          const int s = it % STAGES;
+          if (it >= STAGES && !mbar_wait(&empty_bar[s], ((it / STAGES) - 1) & 1)) {
+            ok = false;
+            s_fail = 1;
+            break;
+          }
+          const int kk = kInt8 ? kb * BK_BYTES : (kb % kb_per_pass) * 64;
+          const CUtensorMap* mb = (kInt8 || kb < kb_per_pass) ? &map_b0 : &map_b1;
+          uint8_t* dst = smem + s * STAGE_BYTES;
+          mbar_expect_tx(&full_bar[s], STAGE_BYTES);
+          tma_load_2d(dst, &map_a, &full_bar[s], kk, m0);
+          tma_load_2d(dst + A_STAGE, mb, &full_bar[s], kk, n0);
+        }
+      }
+    }
+    __syncwarp();
+  } else if (warp == MMA_WARP) {
+    if (lane == 0) {
+      const uint32_t idesc = kInt8 ? kIdescI8 : kIdescBF16;
+      uint32_t it = 0;
+      int i = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
+        const int a = i & 1;
+        if (i >= 2 && !mbar_wait(&acce_bar[a], ((i >> 1) - 1) & 1)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t tmem_d = tmem_base + (uint32_t)(a * BN);
+        for (int kb = 0; kb < kblocks; ++kb, ++it) {
+          const int s = it % STAGES;
+          if (!mbar_wait(&full_bar[s], (it / STAGES) & 1)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
+          const uint32_t b_addr = a_addr + A_STAGE;
+#pragma unroll
+          for (int k = 0; k < BK_BYTES / 32; ++k) {
+            mma<kInt8>(tmem_d, sw128_desc(a_addr + k * 32), sw128_desc(b_addr + k * 32), idesc,
+                       (kb > 0 || k > 0) ? 1u : 0u);
+          }
+          mma_commit(&empty_bar[s]);  // frees the stage once these MMAs have read it
+        }
+        if (ok) mma_commit(&accf_bar[a]);  // accumulator a complete
+      }
+      if (!ok) s_fail = 1;
+    }
+    __syncwarp();
+  } else {
+    // ---- epilogue: warps 2-5, all 128 threads take every branch together ----
+    const int quarter = warp & 3;
+    const int row = quarter * 32 + lane;
+    int i = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+      const int a = i & 1;
+      const int tm = t / ntn, tn = t % ntn;
+      const int b = tm * BM + row, n0 = tn * BN;
+      const bool ready = mbar_wait(&accf_bar[a], (i >> 1) & 1);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      long long qi = 0;
+      double qf = 0.0;
+      if (__all_sync(0xFFFFFFFFu, ready)) {
+        uint32_t xbits[BN / 32];
+        const uint32_t* th = theta + (size_t)(b < shots ? b : 0) * n32;
+#pragma unroll
+        for (int c = 0; c < BN / 32; ++c) {
+          const int j0 = n0 + 32 * c;
+          xbits[c] = (b < shots && j0 < n) ? __ldg(th + (j0 >> 5)) : 0u;
+        }
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 64) {
+          uint32_t rr[64];
+          const uint32_t taddr =
+              tmem_base + (uint32_t)(a * BN) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
+          tmem_load32_nowait(taddr, *reinterpret_cast<uint32_t(*)[32]>(&rr[0]));
+          tmem_load32_nowait(taddr + 32, *reinterpret_cast<uint32_t(*)[32]>(&rr[32]));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int e = 0; e < 64; ++e) {
+            const int j = n0 + c0 + e;
+            const uint32_t bit = (xbits[(c0 + e) >> 5] >> (e & 31)) & 1u;
+            if (j < n) {
+              if constexpr (kInt8) {
+                const int v = (int)rr[e];
+                qi += bit ? v : -v;
+              } else {
+                const double v = (double)__uint_as_float(rr[e]);
+                qf += bit ? v : -v;
+              }
+            }
+          }
+        }
+      } else {
+        s_fail = 1;
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce_bar[a]);  // accumulator a may be overwritten
+      if (b < shots) qpart[(size_t)tn * shots + b] = kInt8 ? (double)qi : qf;
+      __threadfence();
+      epi_barrier();
+      if (quarter == 0 && lane == 0) s_bcast = atomicAdd(&mcount[tm], 1u);
+      epi_barrier();
+      if (s_bcast == (unsigned)(ntn - 1)) {
+        // this CTA wrote the last node tile of candidate block tm
+        __threadfence();
+        uint64_t kbest = 0;
+        if (b < shots) {
+          double q = 0.0;
+          for (int u = 0; u < ntn; ++u) q += __ldcg(qpart + (size_t)u * shots + b);
+          const double val = spin ? -q / 2.0 : (2.0 * upper_sum - q) / 4.0;
+          const float v = (float)val;
+          if (energies) energies[b] = v;
+          kbest = sel_key(v, (uint64_t)b, geo);
+        }
+        kbest = warp_max_u64(kbest);
+        if (lane == 0 && kbest) atomicMax(key, (unsigned long long)kbest);
+        __threadfence();
+        epi_barrier();
+        if (quarter == 0 && lane == 0) {
+          const unsigned done = atomicAdd(mdone, 1u);
+          if (done == (unsigned)(ntm - 1)) {
+            __threadfence();
+            float v;
+            int64_t idx;
+            sel_decode(atomicAdd(key, 0ull), geo, &v, &idx);
+            if (atomicAdd(err, 0) || s_fail) {
+              v = __int_as_float(0x7FC00000);
+              idx = -1;
+            }
+            if (best_energy) *best_energy = v;
+            if (best_index) *best_index = (int)idx;
+          }
+        }
+      }
+      epi_barrier();  // s_bcast is rewritten by the next tile
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == MMA_WARP) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                 "r"(ACC_COLS));
+  }
+  if (threadIdx.x == 0 && s_fail) atomicExch(err, 1);
+}
+
+// +-1 operand from packed bits: X[b][v] for v < 32*ceil(n/32) (row pitch ld
+// elements); columns at and beyond n are never read (the A tensor map ends at n).
+template <typename T>
+__global__ void expand_pm1_kernel(const uint32_t* __restrict__ theta, int shots, int n32, int ld,
+                                  T* __restrict__ X) {
+  const long long total = (long long)shots * n32;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int b = (int)(e / n32), w = (int)(e - (long long)b * n32);
+    const uint32_t bits = theta[e];
+    T* dst = X + (size_t)b * ld + (size_t)w * 32;
+    if constexpr (sizeof(T) == 1) {
+      // bit -> byte 0x01 (set) or 0xFF (clear), four at a time
+      uint32_t o[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const uint32_t t = (((bits >> (4 * q)) & 0xFu) * 0x00204081u) & 0x01010101u;
+        o[q] = 0xFFFFFFFFu - t * 0xFEu;
+      }
+      reinterpret_cast<uint4*>(dst)[0] = make_uint4(o[0], o[1], o[2], o[3]);
+      reinterpret_cast<uint4*>(dst)[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    } else {
+      uint32_t o[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const uint32_t lo = ((bits >> (2 * q)) & 1u) ? 0x3F80u : 0xBF80u;
+        const uint32_t hi = ((bits >> (2 * q + 1)) & 1u) ? 0x3F80u : 0xBF80u;
+        o[q] = lo | (hi << 16);
+      }
+      uint4* d4 = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) d4[q] = make_uint4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+    }
+  }
+}
+
+}  // namespace tc
+
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+  }
+  return fn;
+}
+
+// 2-D K-major map: rows x cols elements (cols contiguous, row pitch `pitch`
+// elements), box = box_rows x (128 bytes of elements), 128-byte swizzle.
+static bool make_map(CUtensorMap* map, const void* base, bool int8, int rows, int cols, int pitch,
+                     int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) return false;
+  const int esz = int8 ? 1 : 2;
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)pitch * esz};
+  cuuint32_t box[2] = {(cuuint32_t)(128 / esz), (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, int8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                   const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+
+struct MapCacheEntry {
+  const void* base;
+  int rows, cols, pitch, box_rows;
+  bool int8;
+  CUtensorMap map;
+};
+
+// Tensor maps depend only on (address, shape): keep the last few encoded.
+static bool cached_map(CUtensorMap* out, const void* base, bool int8, int rows, int cols, int pitch,
+                       int box_rows) {
+  static MapCacheEntry cache[8] = {};
+  static int next = 0;
+  for (const auto& e : cache) {
+    if (e.base == base && e.rows == rows && e.cols == cols && e.pitch == pitch &&
+        e.box_rows == box_rows && e.int8 == int8) {
+      *out = e.map;
+      return true;
+    }
+  }
+  MapCacheEntry e{base, rows, cols, pitch, box_rows, int8, {}};
+  if (!make_map(&e.map, base, int8, rows, cols, pitch, box_rows)) return false;
+  cache[next] = e;
+  next = (next + 1) % 8;
+  *out = e.map;
+  return true;
+}
+
+extern cudaEvent_t g_score_ev_before, g_score_ev_after;
+
+// Tensor-core scoring with the finish and the selection fused in. Returns
+// PQI_ENOTSUP when the device or driver lacks the feature, so the caller can
+// use the CUDA-core path.
+pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int spin,
+                    const SelGeom& geo, float* energies, float* best_energy, int* best_index,
+                    Workspace& ws, cudaStream_t s) {
+  static int arch_ok = -1;
+  static int num_sms = 148;
+  if (arch_ok < 0) {
+    int dev = 0, major = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
+    arch_ok = (major == 10) ? 1 : 0;
+  }
+  if (!arch_ok || !encode_fn()) return PQI_ENOTSUP;
+  const int n = w->n, n32 = (n + 31) >> 5, ld = w->ld;
+  const bool i8 = w->kind == PQI_W_I8;
+  const int ntn = (n + tc::BN - 1) / tc::BN;
+  const int ntm = (shots + tc::BM - 1) / tc::BM;
+  // one zeroed control block: err, mdone, key, then mcount[ntm]
+  const size_t ctl_bytes = 64 + (size_t)ntm * sizeof(unsigned);
+  uint8_t* ctl = ws.take<uint8_t>(ctl_bytes);
+  double* qpart = ws.take<double>((size_t)ntn * shots);
+  void* X = i8 ? (void*)ws.take<int8_t>((size_t)shots * ld)
+               : (void*)ws.take<uint16_t>((size_t)shots * ld);
+  if (!ctl || !qpart || !X) return PQI_EINVAL;
+  int* err = reinterpret_cast<int*>(ctl);
+  unsigned* mdone = reinterpret_cast<unsigned*>(ctl + 8);
+  unsigned long long* key = reinterpret_cast<unsigned long long*>(ctl + 16);
+  unsigned* mcount = reinterpret_cast<unsigned*>(ctl + 64);
+  if (i8) {
+    if (!w->W_i8) return PQI_EINVAL;
+  } else if (!w->W_hi || !w->W_lo) {
+    return PQI_EINVAL;
+  }
+  CUtensorMap ma, mb0, mb1;
+  if (!cached_map(&ma, X, i8, shots, n, ld, tc::BM)) return PQI_ENOTSUP;
+  if (!cached_map(&mb0, i8 ? (const void*)w->W_i8 : (const void*)w->W_hi, i8, n, n, ld, tc::BN))
+    return PQI_ENOTSUP;
+  if (!cached_map(&mb1, i8 ? (const void*)w->W_i8 : (const void*)w->W_lo, i8, n, n, ld, tc::BN))
+    return PQI_ENOTSUP;
+  static bool attr_set[2] = {false, false};
+  if (!attr_set[i8]) {
+    if (i8) {
+      PQI_TRY(cudaFuncSetAttribute(tc::score_tc_kernel<true>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    } else {
+      PQI_TRY(cudaFuncSetAttribute(tc::score_tc_kernel<false>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    }
+    attr_set[i8] = true;
+  }
+  PQI_TRY(cudaMemsetAsync(ctl, 0, ctl_bytes, s));
+  const long long words = (long long)shots * n32;
+  const int eg = (int)std::max<long long>(1, std::min<long long>((words + 255) / 256, 148 * 16));
+  if (i8) {
+    tc::expand_pm1_kernel<int8_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (int8_t*)X);
+  } else {
+    tc::expand_pm1_kernel<uint16_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (uint16_t*)X);
+  }
+  PQI_LAUNCHED("expand_pm1_kernel");
+  const int grid = std::min(ntn * ntm, num_sms);
+  if (g_score_ev_before) PQI_TRY(cudaEventRecord(g_score_ev_before, s));
+  if (i8) {
+    tc::score_tc_kernel<true><<<grid, tc::PTHREADS, tc::SMEM_BYTES, s>>>(
+        ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount, mdone,
+        key, best_energy, best_index, err);
+  } else {
+    tc::score_tc_kernel<false><<<grid, tc::PTHREADS, tc::SMEM_BYTES, s>>>(
+        ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount, mdone,
+        key, best_energy, best_index, err);
+  }
+  PQI_LAUNCHED("score_tc_kernel");
+  if (g_score_ev_after) PQI_TRY(cudaEventRecord(g_score_ev_after, s));
+  return PQI_OK;
+}
+
 }  // namespace pqi
