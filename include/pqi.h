@@ -278,6 +278,40 @@ pqi_status pqi_exact_search(const float* W, int n, int is_spin_glass, double* be
                             void* stream);
 
 /* ---------------------------------------------------------------------------
+ * TFIM-inspired candidate sampler of maxcut_tfim
+ * -------------------------------------------------------------------------*/
+
+/* Per-node J_eff (float64) and degree (uint32) of the caller's n*n W, as
+ * init_J_and_z (maxcut_tfim.py:189-209): an entry counts when W_ij - min(W) >
+ * FLT_EPSILON (float32 difference), J_eff = -(sum of those differences)/degree. */
+pqi_status pqi_tfim_jz(const float* W, int n, double* J_eff, unsigned int* degrees,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* Workspace bytes pqi_tfim_cdf needs. */
+size_t pqi_tfim_cdf_workspace_bytes(int n, int quality);
+
+/* Cumulative Hamming-weight distribution, n-1 float64 entries, as
+ * maxcut_hamming_cdf (maxcut_tfim_util.py:654-687) with
+ * probability_by_hamming_weight and _apply_time_envelope (util:578-651);
+ * thresholds (n+1 float64, init_thresholds of util:558-575) seed the sum. */
+pqi_status pqi_tfim_cdf(const double* J_eff, const unsigned int* degrees, int n, int quality,
+                        double anneal_t, double anneal_h, const double* thresholds, double* cum,
+                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* Workspace bytes pqi_tfim_sample needs for n nodes (large n only). */
+size_t pqi_tfim_sample_workspace_bytes(int n);
+
+/* Draw `shots` candidates as packed bits (shots x ceil(n/32) words): shot s
+ * draws a Hamming-weight index from `cum` (sample_mag, util:691-707) and picks
+ * nodes starting at s % n with weights multiplied by repulsion_base^(-W_kv)
+ * after each pick (local_repulsion_choice, maxcut_tfim.py:36-74; bit_pick,
+ * util:711-724); selected = weight exactly zero. Random draws are a
+ * counter-based function of (seed, round, s, draw). */
+pqi_status pqi_tfim_sample(const float* W, int n, const double* cum, double repulsion_base,
+                           uint64_t seed, uint64_t round, int shots, uint32_t* theta_out,
+                           void* workspace, size_t workspace_bytes, void* stream);
+
+/* ---------------------------------------------------------------------------
  * Objectives, packing
  * -------------------------------------------------------------------------*/
 

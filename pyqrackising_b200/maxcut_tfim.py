@@ -4,12 +4,19 @@ Same signature, defaults and return tuple as the reference
 (``pyqrackising/maxcut_tfim.py:342-422``). Below the heuristic threshold
 (n < 24) the exhaustive search runs on the GPU with the reference's value order
 and tie rule (``pqi_exact_search``); above it the TFIM-inspired sampler draws
-candidate batches that the tensor-core scoring kernel evaluates.
+candidate batches on the GPU (``pqi_tfim_*``) that the tensor-core scoring
+kernel evaluates, round after round while the best value improves, as the
+reference's GPU branch does (``sample_for_opencl``). ``is_maxcut_gpu`` is
+accepted and ignored (no CPU path). The sampler's generator is counter-based
+and seeded (``set_seed``; the reference's is unseeded), so results are
+reproducible for a fixed seed.
 """
 
 from __future__ import annotations
 
 import ctypes
+import math
+import os
 
 import numpy as np
 import torch
@@ -64,4 +71,152 @@ def maxcut_tfim(
             return "0" * n_qubits, 0.0, (nodes, [])
         return bit_string, best_value, (l, r)
 
-    raise NotImplementedError("TFIM sampler not built yet")
+    if quality is None:
+        quality = 6
+    if shots is None:
+        shots = n_qubits << quality
+    if anneal_t is None:
+        anneal_t = 8.0
+    if anneal_h is None:
+        anneal_h = 8.0
+    if repulsion_base is None:
+        repulsion_base = 5.0
+
+    dg = D.DeviceGraph(G_m)
+    best_solution, best_value = sample_and_score(
+        dg, int(quality), int(shots), bool(is_spin_glass), float(anneal_t), float(anneal_h), float(repulsion_base)
+    )
+    bit_string, l, r = get_cut(best_solution, nodes)
+    if best_value < 0.0:
+        return "0" * n_qubits, 0.0, (nodes, [])
+    return bit_string, best_value, (l, r)
+
+
+_seed = None
+
+
+def set_seed(seed: int | None):
+    """Seed of the sampler's counter-based generator (None: a fresh random seed
+    per process, like the reference's unseeded generator)."""
+    global _seed
+    _seed = None if seed is None else int(seed) & 0xFFFFFFFFFFFFFFFF
+
+
+def _current_seed() -> int:
+    global _seed
+    if _seed is None:
+        env = os.getenv("PYQRACKISING_B200_SEED")
+        _seed = int(env) if env else int.from_bytes(os.urandom(8), "little")
+    return _seed
+
+
+def init_thresholds(n_qubits: int) -> np.ndarray:
+    """Initial Hamming-weight weights (maxcut_tfim_util.py:558-575): binomial
+    coefficients, normalised with exact integers on the host. For even n the
+    reference never writes the middle entry of its np.empty array (its value
+    is whatever memory held); here it is 0.0."""
+    n_bias = n_qubits + 1
+    thresholds = np.zeros(n_bias, dtype=np.float64)
+    normalizer = 0
+    for q in range(n_qubits >> 1):
+        normalizer += math.comb(n_qubits, q) << 1
+    if n_qubits & 1:
+        normalizer += math.comb(n_qubits, n_qubits >> 1)
+    p = 1
+    for q in range(n_qubits >> 1):
+        val = p / normalizer
+        thresholds[q] = val
+        thresholds[n_bias - (q + 1)] = val
+        p = math.comb(n_qubits, q + 1)
+    if n_qubits & 1:
+        thresholds[n_qubits >> 1] = p / normalizer
+    return thresholds
+
+
+def hamming_cdf(dg: D.DeviceGraph, quality: int, anneal_t: float, anneal_h: float):
+    """(J_eff, degrees, cum_prob) on the device (init_J_and_z + maxcut_hamming_cdf)."""
+    n = dg.n
+    dev = dg.device
+    lib = _lib.load()
+    J_eff = torch.empty(n, dtype=torch.float64, device=dev)
+    degrees = torch.empty(n, dtype=torch.int32, device=dev)
+    wsp, wsn = dg.wsp(1)
+    _lib.call("pqi_tfim_jz", D._ptr(dg.W), n, D._ptr(J_eff), D._ptr(degrees), wsp, wsn, dg.sp())
+    thr = torch.from_numpy(init_thresholds(n)).to(dev)
+    cum = torch.empty(max(n - 1, 1), dtype=torch.float64, device=dev)
+    ws = dg.ws.get(lib.pqi_tfim_cdf_workspace_bytes(n, quality))
+    _lib.call(
+        "pqi_tfim_cdf",
+        D._ptr(J_eff),
+        D._ptr(degrees),
+        n,
+        int(quality),
+        float(anneal_t),
+        float(anneal_h),
+        D._ptr(thr),
+        D._ptr(cum),
+        ws[0],
+        ws[1],
+        dg.sp(),
+    )
+    return J_eff, degrees, cum
+
+
+def sample_batch(dg: D.DeviceGraph, cum, shots: int, repulsion_base: float, seed: int, round_: int, out=None):
+    """One round of shot_loop (maxcut_tfim.py:139-145) on the device: `shots`
+    candidates as packed words [shots, ceil(n/32)]."""
+    n = dg.n
+    lib = _lib.load()
+    if out is None:
+        out = torch.empty(shots * dg.n32 + 1, dtype=torch.int32, device=dg.device)
+        out[-1] = 0  # spare word (single-row 64-bit view), never written by the sampler
+    ws = dg.ws.get(lib.pqi_tfim_sample_workspace_bytes(n))
+    _lib.call(
+        "pqi_tfim_sample",
+        D._ptr(dg.W),
+        n,
+        D._ptr(cum),
+        float(repulsion_base),
+        ctypes.c_uint64(seed),
+        ctypes.c_uint64(round_),
+        int(shots),
+        D._ptr(out),
+        ws[0],
+        ws[1],
+        dg.sp(),
+    )
+    return out
+
+
+def sample_and_score(dg: D.DeviceGraph, quality: int, shots: int, is_spin_glass: bool, anneal_t: float,
+                     anneal_h: float, repulsion_base: float, max_rounds: int = 1 << 20):
+    """sample_for_opencl (maxcut_tfim.py:148-186) on the device: draw rounds of
+    candidates and score each round with the batched scoring kernel until a
+    round does not beat the best so far. Returns (bool[n], value)."""
+    n = dg.n
+    _, _, cum = hamming_cdf(dg, quality, anneal_t, anneal_h)
+    shots = ((max(1, shots >> 1) + 31) >> 5) << 5
+    mpe = D.max_gpu_proc_elem(dg.device)
+    G, L = D.geometry(shots, shots, mpe)
+    best_solution = np.zeros(n, dtype=np.bool_)
+    if is_spin_glass:
+        _, en = dg.rescore(dg.pack(best_solution))
+        best_energy = float(en.item())
+    else:
+        best_energy = 0.0
+    seed = _current_seed()
+    buf = None
+    for round_ in range(max_rounds):
+        buf = sample_batch(dg, cum, shots, repulsion_base, seed, round_, out=buf)
+        _, be, bi = dg.calculate_cut(buf, shots, is_spin_glass, G, L, energies=False)
+        energy = float(be.item())
+        if energy > best_energy:
+            b = int(bi.item())
+            best_energy = float(np.float32(energy))
+            best_solution = dg.unpack(buf[b * dg.n32 : (b + 1) * dg.n32])[0]
+        else:
+            break
+    if is_spin_glass:
+        cut, _ = dg.rescore(dg.pack(best_solution))
+        best_energy = float(cut.item())
+    return best_solution, float(best_energy)

@@ -168,10 +168,42 @@ def exact_fixtures(mu, mt):
     return d
 
 
+def tfim_fixtures(mu, mt):
+    """The sampler's deterministic parts from the reference's numba code:
+    init_J_and_z and maxcut_hamming_cdf (maxcut_tfim.py:189-209,
+    maxcut_tfim_util.py:654-687). init_thresholds leaves one middle entry of an
+    np.empty array unset; the fixture passes that entry as 0.0 (the value the
+    rebuild uses), so the reference function sees a defined input. Also the
+    reference's own maxcut_tfim results (unseeded) over repeated runs."""
+    import importlib
+
+    ours = importlib.import_module("pyqrackising_b200.maxcut_tfim")
+    d = {}
+    for name, W, spin in (("c1", wl.regular_pm1(64, seed=42), True), ("c2", wl.erdos_renyi(256, 0.5, seed=1), False)):
+        n = W.shape[0]
+        J_eff, degrees = mt.init_J_and_z(W, 5.0)
+        d[f"{name}_W"] = W
+        d[f"{name}_J_eff"] = J_eff
+        d[f"{name}_degrees"] = degrees
+        for q in (2, 6):
+            thr = ours.init_thresholds(n)
+            d[f"{name}_thresholds"] = thr.copy()
+            d[f"{name}_cum_q{q}"] = mu.maxcut_hamming_cdf(thr, n, J_eff, degrees, q, 8.0, 8.0)
+        runs = [mt.maxcut_tfim(W, quality=6 if n <= 64 else 2, is_spin_glass=spin) for _ in range(8)]
+        bits = [np.array([c == "1" for c in r[0]]) for r in runs]
+        d[f"{name}_ref_runs_cut"] = np.array([O.compute_cut(b, W) for b in bits])
+        d[f"{name}_ref_runs_energy"] = np.array([O.compute_energy(b, W) for b in bits])
+    return d
+
+
 def main():
     if not O.ref_available():
         O.build_ref(REFERENCE)
     mu, mt, sg = ref_modules()
+    if "--tfim-only" in sys.argv:
+        np.savez_compressed(os.path.join(OUT, "golden_tfim.npz"), **tfim_fixtures(mu, mt))
+        return
+    np.savez_compressed(os.path.join(OUT, "golden_tfim.npz"), **tfim_fixtures(mu, mt))
     for name, W, spin in instances():
         d = make_instance(name, W, spin, mu, mt, sg)
         np.savez_compressed(os.path.join(OUT, f"golden_{name}.npz"), **d)

@@ -55,3 +55,24 @@ def test_small_n_paths():
     assert spin_glass_solver(np.zeros((1, 1), np.float32))[0] == "0"
     W2 = np.array([[0, 2.5], [2.5, 0]], np.float32)
     assert spin_glass_solver(W2)[:2] == ("01", np.float32(2.5))
+
+
+@pytest.mark.parametrize("name", ["c1_regular64", "c4_reg100"])
+def test_spin_glass_solver_without_best_guess(name, oracle_mod):
+    """The full drop-in path: GPU sampler seed (maxcut_tfim) then local search."""
+    import importlib
+
+    from pyqrackising_b200 import spin_glass_solver
+
+    MT = importlib.import_module("pyqrackising_b200.maxcut_tfim")
+    d = load_golden(name)
+    W = d["W"]
+    MT.set_seed(5)
+    try:
+        bs, cut, _, energy = spin_glass_solver(W, quality=4, is_spin_glass=True)
+    finally:
+        MT.set_seed(None)
+    bits = np.array([c == "1" for c in bs], dtype=bool)
+    assert energy == pytest.approx(-oracle_mod.compute_energy(bits, W), rel=1e-12, abs=1e-9)
+    # a 2-opt local optimum at least as good as 90% of the reference run from its own seed
+    assert -energy <= 1e-9 or oracle_mod.compute_energy(bits, W) >= 0.9 * float(d["e2e_energy"])

@@ -1,0 +1,115 @@
+"""The GPU TFIM sampler behind maxcut_tfim against the reference's numba code:
+init_J_and_z and maxcut_hamming_cdf value by value, the sampler's invariants
+and its Hamming-weight distribution, and end-to-end cut quality against the
+reference's own (unseeded) runs."""
+
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+MT = importlib.import_module("pyqrackising_b200.maxcut_tfim")
+
+
+def _sample_mag(cum, p):
+    """maxcut_tfim_util.py:691-707, with the same 64-probe cap as the kernel."""
+    left, right, m = 0, len(cum) - 1, 0
+    for _ in range(64):
+        m = (left + right) >> 1
+        if cum[m] >= p and (m == 0 or cum[m - 1] < p):
+            break
+        if cum[m] < p:
+            left = m + 1
+        else:
+            right = m - 1
+    return m
+
+
+def _dg(W):
+    from pyqrackising_b200.device import DeviceGraph
+
+    return DeviceGraph(W)
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_jz_and_cdf_match_reference(name):
+    d = load_golden("tfim")
+    W = d[f"{name}_W"]
+    dg = _dg(W)
+    for q in (2, 6):
+        J_eff, degrees, cum = MT.hamming_cdf(dg, q, 8.0, 8.0)
+        assert np.array_equal(degrees.cpu().numpy().astype(np.uint32), d[f"{name}_degrees"])
+        np.testing.assert_allclose(J_eff.cpu().numpy(), d[f"{name}_J_eff"], rtol=1e-12, atol=1e-12)
+        np.testing.assert_allclose(cum.cpu().numpy(), d[f"{name}_cum_q{q}"], rtol=1e-9, atol=1e-12)
+
+
+def test_sampler_invariants_and_weight_distribution():
+    d = load_golden("tfim")
+    W = d["c1_W"]  # 3-regular: repulsion never underflows a weight to zero
+    n = W.shape[0]
+    dg = _dg(W)
+    _, _, cum = MT.hamming_cdf(dg, 6, 8.0, 8.0)
+    shots = 1 << 15
+    words = MT.sample_batch(dg, cum, shots, 5.0, seed=1234, round_=0)
+    bits = dg.unpack(words, rows=shots)
+    counts = bits.sum(axis=1)
+    s = np.arange(shots)
+    assert np.all(bits[s, s % n]), "the first pick is node s % n"
+    # popcount k <-> Hamming-weight index m: k == 1 <=> m == 1; k == 2 <=> m in {0, 2}; else k == m
+    c = d["c1_cum_q6"]
+    expect = np.zeros(n + 1)
+    grid = (np.arange(20000) + 0.5) / 20000
+    for p in grid:  # the reference's bisection (sample_mag) over a fine grid of p
+        m = _sample_mag(c, p)
+        expect[2 if m == 0 else m] += 1.0 / len(grid)
+    got = np.bincount(counts, minlength=n + 1) / shots
+    assert 0.5 * np.abs(got - expect).sum() < 0.02  # total variation distance
+    # same seed and round -> same batch; another round -> another batch
+    again = MT.sample_batch(dg, cum, shots, 5.0, seed=1234, round_=0)
+    assert torch.equal(words, again)
+    other = MT.sample_batch(dg, cum, shots, 5.0, seed=1234, round_=1)
+    assert not torch.equal(words, other)
+
+
+def test_repulsion_lowers_neighbour_selection():
+    """Nodes adjacent to the first pick are selected less often than others."""
+    d = load_golden("tfim")
+    W = np.abs(d["c1_W"])  # unit weights on the same 3-regular graph
+    n = W.shape[0]
+    dg = _dg(W)
+    _, _, cum = MT.hamming_cdf(dg, 6, 8.0, 8.0)
+    shots = 1 << 15
+    bits = dg.unpack(MT.sample_batch(dg, cum, shots, 5.0, seed=7, round_=0), rows=shots)
+    s = np.arange(shots)
+    first = s % n
+    nb = W[first] > 0
+    others = ~nb
+    others[s, first] = False
+    # selection rates over ~1e5 / ~2e6 samples: standard errors ~1e-3
+    assert bits[nb].mean() < bits[others].mean() - 0.02
+
+
+@pytest.mark.parametrize("name", ["c1", "c2"])
+def test_maxcut_tfim_end_to_end_quality(name):
+    d = load_golden("tfim")
+    W = d[f"{name}_W"]
+    spin = name == "c1"
+    q = 6 if W.shape[0] <= 64 else 2
+    from oracle import oracle as O
+
+    vals = []
+    for seed in range(4):
+        MT.set_seed(seed)
+        bs, cut, (l, r) = MT.maxcut_tfim(W, quality=q, is_spin_glass=spin)
+        bits = np.array([ch == "1" for ch in bs])
+        assert cut == pytest.approx(O.compute_cut(bits, W), rel=1e-12, abs=1e-9)
+        assert len(l) + len(r) == W.shape[0]
+        vals.append(cut)
+    MT.set_seed(None)
+    ref = d[f"{name}_ref_runs_cut"]
+    assert np.mean(vals) >= np.mean(ref) - 2.0 * np.std(ref) - 1e-9
