@@ -278,6 +278,37 @@ pqi_status pqi_exact_search(const float* W, int n, int is_spin_glass, double* be
                             void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Batched local search (many graphs x many starting states, one launch)
+ * -------------------------------------------------------------------------*/
+
+/* Size of one graph descriptor in the device array pqi_batch_search reads:
+ * {const void* W (prepared W_i8 or W_f32z); int n; int ld; int kind; int pad;
+ *  double upper_sum}. */
+size_t pqi_batch_graph_desc_bytes(void);
+
+/*
+ * Iterated local search for `tasks` (graph, starting state) pairs in one
+ * persistent launch. Task t uses graph task_graph[t] and starts from
+ * init_states + t*words_pitch (ceil(n/32) words). Per task: rounds+1 steepest
+ * single-flip ascents (largest gain, lowest node on ties, while > 0, at most
+ * flip_budget flips each) separated by `kick` forced flips per round, drawn
+ * uniformly or, when kick_cdf is given, from the graph's proposal distribution
+ * (normalised cumulative array at kick_cdf + cdf_offset[graph]). Writes the
+ * best state (best_states + t*words_pitch) and value (cut, or the spin energy
+ * sum_{u<v} W_uv (s_u != s_v ? 1 : -1) when is_spin_glass) of each task, adds
+ * the flips made to *flips_total and sets *status to PQI_ETIMEOUT if a flip
+ * budget ran out. All graphs of a launch share `kind`; max_n bounds their n.
+ * No reference counterpart: it batches the single-graph loop of
+ * spin_glass_solver.py:603-717.
+ */
+pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_graph,
+                            const uint32_t* init_states, int words_pitch, int tasks, int max_n,
+                            int kind, int is_spin_glass, int rounds, int kick, int flip_budget,
+                            uint64_t seed, const double* kick_cdf, const long long* cdf_offset,
+                            uint32_t* best_states, double* best_values,
+                            unsigned long long* flips_total, int* status, void* stream);
+
+/* ---------------------------------------------------------------------------
  * TFIM-inspired candidate sampler of maxcut_tfim
  * -------------------------------------------------------------------------*/
 

@@ -456,3 +456,32 @@ def spin_glass_gpu_path(W, best_theta, is_spin_glass, gray_iterations, mpe, gray
             theta = st
             improved = True
     return theta, float(max_energy)
+
+
+# --------------------------------------------------------------------------------------
+# Batched form (no reference counterpart): steepest single-flip ascent with the
+# batched kernel's rule -- the largest gain rounded to float32, lowest node on
+# ties, accept while > 0 -- with float64 gains kept incrementally.
+
+
+def steepest_ascent(W, bits, budget=None):
+    """Returns (final bool[n], number of flips)."""
+    Wd = np.asarray(W, dtype=np.float64).copy()
+    np.fill_diagonal(Wd, 0.0)
+    s = np.array(bits, dtype=np.bool_, copy=True)
+    x = np.where(s, 1.0, -1.0)
+    g = x * (Wd @ x)
+    flips = 0
+    budget = budget if budget is not None else 4 * len(s) + 64
+    while True:
+        g32 = g.astype(np.float32)
+        k = int(np.argmax(g32))
+        if not g32[k] > 0 or flips >= budget:
+            break
+        xk = x[k]
+        g -= 2.0 * x * xk * Wd[k]
+        g[k] = -g[k] - 2.0 * xk * xk * Wd[k, k]
+        x[k] = -xk
+        s[k] = not s[k]
+        flips += 1
+    return s, flips

@@ -92,6 +92,8 @@ SIGNATURES = {
     "pqi_gray": (_i, [_WP, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_single_descent": (_i, [_WP, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _sz, _vp]),
     "pqi_apply_flip": (_i, [_WP, _vp, _vp, _i, _i, _vp]),
+    "pqi_batch_graph_desc_bytes": (_sz, []),
+    "pqi_batch_search": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "pqi_tfim_jz": (_i, [_vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_tfim_cdf_workspace_bytes": (_sz, [_i, _i]),
     "pqi_tfim_cdf": (_i, [_vp, _vp, _i, _i, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _sz, _vp]),

@@ -37,18 +37,31 @@ __device__ __forceinline__ int bit_of<uint32_t>(const uint32_t* bits, int v) {
 // gains, then one thread toggles the bit. Must be reached by all threads of
 // the block with the same k. Caller guarantees a barrier after its own reads
 // of g[k] / bits.
-template <typename GT, typename WT, typename W64>
+template <typename GT, typename WT, typename W64, int CH = 16>
 __device__ __forceinline__ void block_flip(GT* g, W64* bits, const WT* __restrict__ Wp, int ld,
                                            int n, int k) {
   const int xk = bit_of<W64>(bits, k);
-  const WT* row = Wp + (size_t)k * ld;
+  const WT* __restrict__ row = Wp + (size_t)k * ld;
   __syncthreads();
-  for (int v = threadIdx.x; v < n; v += blockDim.x) {
-    if (v == k) {
-      g[v] = -g[v];
-    } else {
-      const GT w2 = (GT)2 * (GT)row[v];
-      g[v] += (bit_of<W64>(bits, v) == xk) ? -w2 : w2;
+  // row read in chunks of CH per thread, loads issued before the gains change
+  for (int base = threadIdx.x; base < n; base += CH * blockDim.x) {
+    WT w[CH];
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+      const int v = base + i * blockDim.x;
+      w[i] = v < n ? __ldg(row + v) : (WT)0;
+    }
+#pragma unroll
+    for (int i = 0; i < CH; ++i) {
+      const int v = base + i * blockDim.x;
+      if (v < n) {
+        if (v == k) {
+          g[v] = -g[v];
+        } else {
+          const GT w2 = (GT)2 * (GT)w[i];
+          g[v] += (bit_of<W64>(bits, v) == xk) ? -w2 : w2;
+        }
+      }
     }
   }
   __syncthreads();
@@ -204,7 +217,7 @@ __global__ void __launch_bounds__(1024) descent_kernel(
     esum += (double)val;
     if (threadIdx.x == 0 && trace) trace[cnt] = (int)idx;
     ++cnt;
-    block_flip<double, WT, uint32_t>(g, bits, Wp, ld, n, (int)idx);
+    block_flip<double, WT, uint32_t, 8>(g, bits, Wp, ld, n, (int)idx);
   }
   for (int q = threadIdx.x; q < n32; q += blockDim.x) theta[q] = bits[q];
   if (gains_in_smem)
