@@ -309,6 +309,47 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
                             unsigned long long* flips_total, int* status, void* stream);
 
 /* ---------------------------------------------------------------------------
+ * Learned flip-proposal network (no reference counterpart). bf16 storage,
+ * float32 accumulation. Pointers typed void* hold bf16 (__nv_bfloat16) data.
+ * -------------------------------------------------------------------------*/
+
+/* C[M x N] = alpha op(A) op(B) + beta C32 + bias, optional ReLU; op(X) = X^T when
+ * the trans flag is set (A is then K x M with pitch lda, B is N x K with pitch
+ * ldb). Writes C32 (float32) and/or C16 (bf16) with pitch ldc. */
+pqi_status pqi_mpnn_gemm(int transA, int transB, int M, int N, int K, float alpha, const void* A,
+                         int lda, const void* B, int ldb, float beta, float* C32, void* C16,
+                         int ldc, const float* bias, int relu, void* stream);
+
+/* A_hat = D^-1/2 W D^-1/2 in bf16 (n x ld, zero diagonal and padding) and
+ * s_v = sum_{u != v} |W_vu| (float32) from the caller's n x n W. */
+pqi_status pqi_mpnn_norm_adj(const float* W, int n, void* Ahat, int ld, float* s, void* stream);
+
+/* Node features of a state, bf16 n x 4: [x_v, g_v / s_v, s_v / mean_s, 1]. */
+pqi_status pqi_mpnn_features(const uint32_t* theta, const double* gains64, const float* s,
+                             float mean_s, int n, void* F, void* stream);
+
+/* Softmax of n logits: *loss = -sum_v t_v log p_v, dlogits = p - t, prob = p
+ * (each output and target nullable). One block. */
+pqi_status pqi_mpnn_softmax_xent(const float* logits, const float* target, int n, float* loss,
+                                 float* dlogits, float* prob, void* stream);
+
+/* dZ = dY * (Y > 0) (Y the ReLU output), float32 and optional bf16 copy. */
+pqi_status pqi_mpnn_relu_bwd(const float* dY, const float* Y, size_t count, float* dZ, void* dZ16,
+                             void* stream);
+
+/* out[c] (+)= sum over rows of X[r*ld + c] (bias gradients). */
+pqi_status pqi_mpnn_colsum(const float* X, int rows, int cols, int ld, float* out,
+                           int accumulate, void* stream);
+
+/* float32 -> bf16. */
+pqi_status pqi_mpnn_to_bf16(const float* x, size_t count, void* y, void* stream);
+
+/* One Adam step on float32 master weights w (bias-corrected, step >= 1), with
+ * a bf16 copy written to w16 (nullable). */
+pqi_status pqi_mpnn_adam(float* w, const float* g, float* m, float* v, void* w16, size_t count,
+                         float lr, float b1, float b2, float eps, int step, void* stream);
+
+/* ---------------------------------------------------------------------------
  * TFIM-inspired candidate sampler of maxcut_tfim
  * -------------------------------------------------------------------------*/
 

@@ -94,6 +94,14 @@ SIGNATURES = {
     "pqi_apply_flip": (_i, [_WP, _vp, _vp, _i, _i, _vp]),
     "pqi_batch_graph_desc_bytes": (_sz, []),
     "pqi_batch_search": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pqi_mpnn_gemm": (_i, [_i, _i, _i, _i, _i, ctypes.c_float, _vp, _i, _vp, _i, ctypes.c_float, _vp, _vp, _i, _vp, _i, _vp]),
+    "pqi_mpnn_norm_adj": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
+    "pqi_mpnn_features": (_i, [_vp, _vp, _vp, ctypes.c_float, _i, _vp, _vp]),
+    "pqi_mpnn_softmax_xent": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp]),
+    "pqi_mpnn_relu_bwd": (_i, [_vp, _vp, _sz, _vp, _vp, _vp]),
+    "pqi_mpnn_colsum": (_i, [_vp, _i, _i, _i, _vp, _i, _vp]),
+    "pqi_mpnn_to_bf16": (_i, [_vp, _sz, _vp, _vp]),
+    "pqi_mpnn_adam": (_i, [_vp, _vp, _vp, _vp, _vp, _sz, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _i, _vp]),
     "pqi_tfim_jz": (_i, [_vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_tfim_cdf_workspace_bytes": (_sz, [_i, _i]),
     "pqi_tfim_cdf": (_i, [_vp, _vp, _i, _i, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _sz, _vp]),
