@@ -308,6 +308,22 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
                             uint32_t* best_states, double* best_values,
                             unsigned long long* flips_total, int* status, void* stream);
 
+/*
+ * Steepest single-flip ascent (rounds = 0 of pqi_batch_search: same selection
+ * rule, same trajectory, same outputs and status) with one thread-block
+ * cluster of cluster_size CTAs (2, 4, 8 or 16) per task: the task's nodes are
+ * split over the cluster's CTAs, whose local fields stay on chip, and the
+ * per-flip argmax is exchanged through distributed shared memory. Lower
+ * latency per flip than one CTA per task for large n; max_n must satisfy
+ * ceil(max_n / cluster_size) <= 8192 nodes per CTA. No reference counterpart:
+ * it is the single-flip descent of spin_glass_solver.py:603-717 on a cluster.
+ */
+pqi_status pqi_cluster_ascent(const void* graphs, int num_graphs, const int* task_graph,
+                              const uint32_t* init_states, int words_pitch, int tasks, int max_n,
+                              int kind, int is_spin_glass, int cluster_size, int flip_budget,
+                              uint32_t* best_states, double* best_values,
+                              unsigned long long* flips_total, int* status, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Learned flip-proposal network (no reference counterpart). bf16 storage,
  * float32 accumulation. Pointers typed void* hold bf16 (__nv_bfloat16) data.

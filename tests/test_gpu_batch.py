@@ -88,3 +88,54 @@ def test_proposal_distribution_kicks():
     v0, _, _, _ = bs.run(task_graph, words, 1, rounds=0)
     assert int(status.item()) == 0
     assert torch.all(v >= v0)
+
+
+@pytest.mark.parametrize("kind", ["int", "float"])
+@pytest.mark.parametrize("csize", [2, 8, 16])
+def test_cluster_ascent_matches_oracle(kind, csize, oracle_mod):
+    """One thread-block cluster per task: the same states, values and flip
+    counts as the oracle's steepest ascent (and hence as the batched kernel),
+    on uneven graphs including sizes that leave CTAs of a cluster idle."""
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    O = oracle_mod
+    Ws = _graphs(kind, [64, 100, 257, 190, 1000, 3000], seed=5)
+    dgs = [DeviceGraph(W) for W in Ws]
+    bs = BatchedSearch(dgs)
+    rng = np.random.default_rng(2)
+    task_graph = [5, 0, 1, 2, 3, 4, 4, 2, 0, 5]
+    states = [rng.random(Ws[g].shape[0]) < 0.5 for g in task_graph]
+    words = bs.pack_states(task_graph, states)
+    for spin in (0, 1):
+        vals, best, flips, status = bs.cluster_ascent(task_graph, words, spin, cluster_size=csize)
+        assert int(status.item()) == 0
+        got = bs.unpack(best, task_graph)
+        total = 0
+        for t, g in enumerate(task_graph):
+            ref, nf = O.steepest_ascent(Ws[g], states[t])
+            total += nf
+            assert np.array_equal(got[t], ref), (t, g)
+            exact = O.compute_energy(got[t], Ws[g]) if spin else O.compute_cut(got[t], Ws[g])
+            assert float(vals[t]) == pytest.approx(exact, rel=1e-9, abs=1e-6)
+        assert int(flips.item()) == total
+        bvals, bbest, bflips, _ = bs.run(task_graph, words, spin, rounds=0)
+        assert torch.equal(bbest, best)
+        assert int(bflips.item()) == int(flips.item())
+
+
+def test_cluster_ascent_flip_budget_reports_timeout():
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+    from pyqrackising_b200 import workloads as wl
+
+    W = wl.sherrington_kirkpatrick(2048, seed=4)
+    bs = BatchedSearch([DeviceGraph(W)])
+    words = bs.random_states([0, 0], seed=3)
+    vals, best, flips, status = bs.cluster_ascent([0, 0], words, 1, cluster_size=4, flip_budget=5)
+    assert int(status.item()) == 3  # PQI_ETIMEOUT
+    bvals, bbest, bflips, bstatus = bs.run([0, 0], words, 1, rounds=0, flip_budget=5)
+    assert int(bstatus.item()) == 3
+    assert torch.equal(bbest, best)
+    assert int(flips.item()) == int(bflips.item()) == 10
+    assert torch.allclose(vals, bvals, rtol=1e-12, atol=1e-9)
