@@ -126,6 +126,10 @@ pqi_status pqi_score_set_path(int path);
  * NULL to stop). Process-wide; lets a caller time the GEMM kernel alone. */
 pqi_status pqi_score_set_events(void* before, void* after);
 
+/* Number of CTAs of the persistent tensor-core scoring kernel (0 = one per SM,
+ * the default). Process-wide; a tuning knob for the scoring autotuner. */
+pqi_status pqi_score_set_grid(int ctas);
+
 /* ---------------------------------------------------------------------------
  * Kernel-level replacements of the reference's OpenCL kernels
  * -------------------------------------------------------------------------*/

@@ -82,6 +82,7 @@ SIGNATURES = {
     "pqi_prepare_weights": (_i, [_vp, _i, ctypes.POINTER(PqiWeightStats), _vp, _vp, _vp, _vp, _WP, _vp]),
     "pqi_score_set_path": (_i, [_i]),
     "pqi_score_set_events": (_i, [_vp, _vp]),
+    "pqi_score_set_grid": (_i, [_i]),
     "pqi_calculate_cut": (_i, [_WP, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _sz, _vp]),
     "pqi_gains": (_i, [_WP, _vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_select": (_i, [_vp, _l, _i, _i, _vp, _vp, _vp, _sz, _vp]),

@@ -159,6 +159,10 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
 // Optional events recorded around the scoring GEMM launch (bench timing).
 cudaEvent_t g_score_ev_before = nullptr, g_score_ev_after = nullptr;
 
+// Set by pqi_score_set_grid: CTAs of the persistent tensor-core scoring kernel
+// (0 = one per SM).
+int g_score_grid = 0;
+
 }  // namespace pqi
 
 using namespace pqi;
@@ -174,6 +178,12 @@ pqi_status pqi_score_set_path(int path) {
 pqi_status pqi_score_set_events(void* before, void* after) {
   g_score_ev_before = reinterpret_cast<cudaEvent_t>(before);
   g_score_ev_after = reinterpret_cast<cudaEvent_t>(after);
+  return PQI_OK;
+}
+
+pqi_status pqi_score_set_grid(int ctas) {
+  if (ctas < 0) return PQI_EINVAL;
+  g_score_grid = ctas;
   return PQI_OK;
 }
 

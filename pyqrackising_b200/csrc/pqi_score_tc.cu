@@ -132,6 +132,18 @@ __device__ __forceinline__ void tmem_load32_nowait(uint32_t taddr, uint32_t (&r)
       : "r"(taddr));
 }
 
+// After tcgen05.wait::ld: ties 32 registers written by an asynchronous
+// tcgen05.ld to this point, so no use of them is scheduled before the wait.
+__device__ __forceinline__ void reg_fence32(uint32_t (&r)[32]) {
+  asm volatile(""
+               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
+                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
+                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
+                 "+r"(r[30]), "+r"(r[31]));
+}
+
 __device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
@@ -168,11 +180,13 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
 
 __device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
-// Persistent scoring kernel: CTA c handles tiles c, c + gridDim.x, ...; tile t
-// covers candidates [128 * (t / ntn), +128) x nodes [256 * (t % ntn), +256).
-// The last CTA to finish a candidate block sums that block's node-tile
-// partials in a fixed order, converts q to the reference's value and folds it
-// into the selection key; the last candidate block decodes the selection.
+// Persistent scoring kernel: CTA c handles the contiguous tiles
+// [c * T / grid, (c + 1) * T / grid); tile t covers candidates
+// [128 * (t / ntn), +128) x nodes [256 * (t % ntn), +256). A CTA that owns a
+// whole candidate block keeps q in registers across its node tiles; a block
+// split between two CTAs goes through per-tile partials summed in tile order
+// by the CTA that completes it. The finisher converts q to the reference's
+// value and folds it into the selection key; the last block decodes it.
 template <bool kInt8>
 __global__ void __launch_bounds__(PTHREADS, 1)
     score_tc_kernel(const __grid_constant__ CUtensorMap map_a,
@@ -199,6 +213,10 @@ __global__ void __launch_bounds__(PTHREADS, 1)
   const int ntn = (n + BN - 1) / BN;
   const int ntm = (shots + BM - 1) / BM;
   const int ntiles = ntn * ntm;
+  // each CTA walks one contiguous chunk of tiles (candidate-block major), so
+  // most blocks are finished by one CTA with q kept in registers
+  const int t_begin = (int)(((long long)blockIdx.x * ntiles) / gridDim.x);
+  const int t_end = (int)(((long long)(blockIdx.x + 1) * ntiles) / gridDim.x);
   const int kb_per_pass = kInt8 ? (n + BK_BYTES - 1) / BK_BYTES : (n + 63) / 64;
   const int kblocks = kInt8 ? kb_per_pass : 2 * kb_per_pass;
 
@@ -230,7 +248,7 @@ __global__ void __launch_bounds__(PTHREADS, 1)
     if (lane == 0) {
       uint32_t it = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+      for (int t = t_begin; t < t_end && ok; ++t) {
         const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
         for (int kb = 0; kb < kblocks; ++kb, ++it) {
           const int s = it % STAGES;
@@ -255,7 +273,7 @@ __global__ void __launch_bounds__(PTHREADS, 1)
       uint32_t it = 0;
       int i = 0;
       bool ok = true;
-      for (int t = blockIdx.x; t < ntiles && ok; t += gridDim.x, ++i) {
+      for (int t = t_begin; t < t_end && ok; ++t, ++i) {
         const int a = i & 1;
         if (i >= 2 && !mbar_wait(&acce_bar[a], ((i >> 1) - 1) & 1)) {
           ok = false;
@@ -288,45 +306,101 @@ __global__ void __launch_bounds__(PTHREADS, 1)
     // ---- epilogue: warps 2-5, all 128 threads take every branch together ----
     const int quarter = warp & 3;
     const int row = quarter * 32 + lane;
+    // q of this thread's candidate over the CTA's tiles of the current block
+    long long qacc_i = 0;
+    double qacc_f = 0.0;
     int i = 0;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++i) {
+    for (int t = t_begin; t < t_end; ++t, ++i) {
       const int a = i & 1;
       const int tm = t / ntn, tn = t % ntn;
       const int b = tm * BM + row, n0 = tn * BN;
-      const bool ready = mbar_wait(&accf_bar[a], (i >> 1) & 1);
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      long long qi = 0;
-      double qf = 0.0;
-      if (__all_sync(0xFFFFFFFFu, ready)) {
-        uint32_t xbits[BN / 32];
+      // this CTA's share of candidate block tm: whole, or split with a neighbour
+      const int blk0 = tm * ntn;
+      const int first = max(t_begin, blk0), last = min(t_end, blk0 + ntn) - 1;
+      const bool whole = first == blk0 && last == blk0 + ntn - 1;
+      // candidate bits of this tile (independent of the MMAs: load before waiting)
+      uint32_t xbits[BN / 32];
+      {
         const uint32_t* th = theta + (size_t)(b < shots ? b : 0) * n32;
 #pragma unroll
         for (int c = 0; c < BN / 32; ++c) {
           const int j0 = n0 + 32 * c;
           xbits[c] = (b < shots && j0 < n) ? __ldg(th + (j0 >> 5)) : 0u;
         }
+      }
+      // columns beyond n hold zeros (TMA zero fill of W), so no column mask
+      const bool ready = mbar_wait(&accf_bar[a], (i >> 1) & 1);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      long long qt_i = 0;
+      double qt_f = 0.0;
+      if (__all_sync(0xFFFFFFFFu, ready)) {
+        const uint32_t tbase =
+            tmem_base + (uint32_t)(a * BN) + ((uint32_t)(quarter * 32) << 16);
+        // rounds of RC columns, the next round's load in flight while one is
+        // summed (64 columns for int8, 32 for float)
+        constexpr int RC = kInt8 ? 64 : 32;
+        uint32_t r0[RC], r1[RC];
 #pragma unroll
-        for (int c0 = 0; c0 < BN; c0 += 64) {
-          uint32_t rr[64];
-          const uint32_t taddr =
-              tmem_base + (uint32_t)(a * BN) + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
-          tmem_load32_nowait(taddr, *reinterpret_cast<uint32_t(*)[32]>(&rr[0]));
-          tmem_load32_nowait(taddr + 32, *reinterpret_cast<uint32_t(*)[32]>(&rr[32]));
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        for (int h = 0; h < RC / 32; ++h)
+          tmem_load32_nowait(tbase + 32 * h, *reinterpret_cast<uint32_t(*)[32]>(&r0[32 * h]));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-          for (int e = 0; e < 64; ++e) {
-            const int j = n0 + c0 + e;
-            const uint32_t bit = (xbits[(c0 + e) >> 5] >> (e & 31)) & 1u;
-            if (j < n) {
-              if constexpr (kInt8) {
-                const int v = (int)rr[e];
-                qi += bit ? v : -v;
-              } else {
-                const double v = (double)__uint_as_float(rr[e]);
-                qf += bit ? v : -v;
+        for (int h = 0; h < RC / 32; ++h) reg_fence32(*reinterpret_cast<uint32_t(*)[32]>(&r0[32 * h]));
+        // int8: sum_j Y_bj and the sum over x_bj = +1 (|Y| <= 127 n, so 256
+        // columns stay below 2^31 for n <= 65536, the int8 path's limit)
+        int s_all = 0, s_set = 0;
+        double f_q = 0.0;                 // float: sum_j x_bj Y_bj
+#pragma unroll
+        for (int rd = 0; rd < BN / RC; ++rd) {
+          uint32_t(&cur)[RC] = (rd & 1) ? r1 : r0;
+          uint32_t(&nxt)[RC] = (rd & 1) ? r0 : r1;
+          if (rd + 1 < BN / RC) {
+#pragma unroll
+            for (int h = 0; h < RC / 32; ++h)
+              tmem_load32_nowait(tbase + (uint32_t)(RC * (rd + 1) + 32 * h),
+                                 *reinterpret_cast<uint32_t(*)[32]>(&nxt[32 * h]));
+          }
+#pragma unroll
+          for (int h = 0; h < RC / 32; ++h) {
+            const uint32_t xb = xbits[(RC / 32) * rd + h];
+            if constexpr (kInt8) {
+#pragma unroll
+              for (int e = 0; e < 32; ++e) {
+                const uint32_t v = cur[32 * h + e];
+                const uint32_t m = 0u - ((xb >> e) & 1u);  // all ones where x_bj = +1
+                s_all += (int)v;
+                s_set += (int)(v & m);
               }
+            } else {
+              // x_bj Y_bj (sign bit flipped where x_bj = -1), summed pairwise in
+              // float over the 32 columns, then added in double
+              float t[16];
+#pragma unroll
+              for (int e = 0; e < 16; ++e) {
+                const uint32_t s0 = ((xb >> (2 * e)) & 1u) ? 0u : 0x80000000u;
+                const uint32_t s1 = ((xb >> (2 * e + 1)) & 1u) ? 0u : 0x80000000u;
+                t[e] = __uint_as_float(cur[32 * h + 2 * e] ^ s0) +
+                       __uint_as_float(cur[32 * h + 2 * e + 1] ^ s1);
+              }
+#pragma unroll
+              for (int w = 8; w > 0; w >>= 1)
+#pragma unroll
+                for (int e = 0; e < w; ++e) t[e] = t[e] + t[e + w];
+              f_q += (double)t[0];
             }
           }
+          if (rd + 1 < BN / RC) {
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int h = 0; h < RC / 32; ++h)
+              reg_fence32(*reinterpret_cast<uint32_t(*)[32]>(&nxt[32 * h]));
+          }
+        }
+        // int8: sum_j x_bj Y_bj = 2 * (sum over x = +1) - (sum over all)
+        if constexpr (kInt8) {
+          qt_i = 2ll * (long long)s_set - (long long)s_all;
+        } else {
+          qt_f = f_q;
         }
       } else {
         s_fail = 1;
@@ -334,18 +408,41 @@ __global__ void __launch_bounds__(PTHREADS, 1)
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(&acce_bar[a]);  // accumulator a may be overwritten
-      if (b < shots) qpart[(size_t)tn * shots + b] = kInt8 ? (double)qi : qf;
-      __threadfence();
-      epi_barrier();
-      if (quarter == 0 && lane == 0) s_bcast = atomicAdd(&mcount[tm], 1u);
-      epi_barrier();
-      if (s_bcast == (unsigned)(ntn - 1)) {
-        // this CTA wrote the last node tile of candidate block tm
-        __threadfence();
+      bool finish = false;  // this CTA folds block tm into the selection
+      double q = 0.0;
+      if (whole) {
+        qacc_i += qt_i;
+        qacc_f += qt_f;
+        if (t == last) {
+          finish = true;
+          q = kInt8 ? (double)qacc_i : qacc_f;
+          qacc_i = 0;
+          qacc_f = 0.0;
+        }
+      } else {
+        // split block: per-tile partials, summed in tile order by the CTA that
+        // completes the block's tile count
+        if (b < shots) qpart[(size_t)tn * shots + b] = kInt8 ? (double)qt_i : qt_f;
+        if (t == last) {
+          __threadfence();
+          epi_barrier();
+          if (quarter == 0 && lane == 0)
+            s_bcast = atomicAdd(&mcount[tm], (unsigned)(last - first + 1)) +
+                      (unsigned)(last - first + 1);
+          epi_barrier();
+          if (s_bcast == (unsigned)ntn) {
+            __threadfence();
+            finish = true;
+            if (b < shots) {
+              for (int u = 0; u < ntn; ++u) q += __ldcg(qpart + (size_t)u * shots + b);
+            }
+          }
+          epi_barrier();  // s_bcast is rewritten by a later block
+        }
+      }
+      if (finish) {
         uint64_t kbest = 0;
         if (b < shots) {
-          double q = 0.0;
-          for (int u = 0; u < ntn; ++u) q += __ldcg(qpart + (size_t)u * shots + b);
           const double val = spin ? -q / 2.0 : (2.0 * upper_sum - q) / 4.0;
           const float v = (float)val;
           if (energies) energies[b] = v;
@@ -371,7 +468,6 @@ __global__ void __launch_bounds__(PTHREADS, 1)
           }
         }
       }
-      epi_barrier();  // s_bcast is rewritten by the next tile
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -489,6 +585,7 @@ static bool cached_map(CUtensorMap* out, const void* base, bool int8, int rows, 
 }
 
 extern cudaEvent_t g_score_ev_before, g_score_ev_after;
+extern int g_score_grid;
 
 // Tensor-core scoring with the finish and the selection fused in. Returns
 // PQI_ENOTSUP when the device or driver lacks the feature, so the caller can
@@ -508,6 +605,8 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
   if (!arch_ok || !encode_fn()) return PQI_ENOTSUP;
   const int n = w->n, n32 = (n + 31) >> 5, ld = w->ld;
   const bool i8 = w->kind == PQI_W_I8;
+  // the int8 epilogue sums 256 columns of |Y| <= 127 n in 32 bits
+  if (i8 && n > 65536) return PQI_ENOTSUP;
   const int ntn = (n + tc::BN - 1) / tc::BN;
   const int ntm = (shots + tc::BM - 1) / tc::BM;
   // one zeroed control block: err, mdone, key, then mcount[ntm]
@@ -552,7 +651,7 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     tc::expand_pm1_kernel<uint16_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (uint16_t*)X);
   }
   PQI_LAUNCHED("expand_pm1_kernel");
-  const int grid = std::min(ntn * ntm, num_sms);
+  const int grid = std::min(ntn * ntm, g_score_grid > 0 ? g_score_grid : num_sms);
   if (g_score_ev_before) PQI_TRY(cudaEventRecord(g_score_ev_before, s));
   if (i8) {
     tc::score_tc_kernel<true><<<grid, tc::PTHREADS, tc::SMEM_BYTES, s>>>(
