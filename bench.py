@@ -16,8 +16,14 @@ and selected with its tie rule. One step = one batch.
   and reads the (best value, index) pair back.
 * roofline: the scoring GEMM (2*B*n^2 integer ops per launch) against the
   int8 tensor rate, taken as twice the measured dense bf16 rate.
-* cpu_baseline: the oracle's C port of the reference's cut_worker on the
-  host cores (a bounded sample of the batch).
+* cpu_baseline: the reference's calculate_cut compiled for the host (or the
+  oracle's C port of it) on the host cores, over a bounded sample of the batch.
+* time_to_best: the other half of the metric, on the Sherrington-Kirkpatrick
+  spin glass (n = 8192, J ~ N(0,1)/sqrt(n) float32): wall time of the plain
+  GPU form (spin_glass_solver's local-search loop from one start) against the
+  batched form (32 starts, one thread-block cluster each, one launch) until
+  each returns; the batched form must reach the plain form's best energy.
+  Both values are re-scored in float64 and their relative error reported.
 
 Multi-GPU: every rank scores its own batches (weak scaling); the only
 exchange is the max over ranks of the elapsed time.
@@ -76,6 +82,12 @@ class ClockSampler:
         self.samples = []
         self._stop = threading.Event()
         self._proc = None
+
+    def wait_first(self, timeout=3.0):
+        """Block until the first sample arrives (so the timed region is covered)."""
+        t0 = time.perf_counter()
+        while not self.samples and time.perf_counter() - t0 < timeout:
+            time.sleep(0.02)
 
     def __enter__(self):
         try:
@@ -223,6 +235,58 @@ def run_reference(args, rank, world):
     return 0
 
 
+def time_to_best(n=8192, starts=32, cluster=8):
+    """Wall time to the plain GPU form's best energy on SK n=8192 (see module doc)."""
+    import importlib
+
+    import torch
+
+    from pyqrackising_b200 import workloads as wl
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    SG = importlib.import_module("pyqrackising_b200.spin_glass_solver")
+    W = wl.sherrington_kirkpatrick(n, seed=1)
+    dg = DeviceGraph(W)
+    start = np.random.default_rng(0).random(n) < 0.5
+    bs = BatchedSearch([dg])
+    tasks = [0] * starts
+    w0 = bs.random_states(tasks, seed=7)
+    # one untimed run of each form on this graph (module load, workspaces,
+    # first-launch attributes), then the timed runs
+    SG.local_search(dg, start, True, n * n, 148, 148, 0.0)
+    bs.cluster_ascent(tasks, w0, True, cluster_size=cluster)
+    torch.cuda.synchronize()
+
+    t0 = time.perf_counter()
+    words, _ = SG.local_search(dg, start, True, n * n, 148, 148, 0.0)
+    _, e_plain = dg.rescore(words)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    e_plain = float(e_plain.item())
+
+    t0 = time.perf_counter()
+    vals, best, flips, status = bs.cluster_ascent(tasks, w0, True, cluster_size=cluster)
+    t_best = int(torch.argmax(vals).item())
+    torch.cuda.synchronize()
+    t_batched = time.perf_counter() - t0
+    e_batched = float(vals[t_best].item())
+    _, e64 = dg.rescore(best[t_best].contiguous())
+    e64 = float(e64.item())
+    return {
+        "workload": f"SK n={n}, J~N(0,1)/sqrt(n) float32, is_spin_glass; plain: local-search loop from 1 start; batched: {starts} starts, cluster ascent ({cluster} CTAs per start)",
+        "plain_s": t_plain,
+        "plain_energy": e_plain,
+        "batched_s": t_batched,
+        "batched_energy": e_batched,
+        "batched_energy_rel_err_vs_fp64": abs(e_batched - e64) / max(abs(e64), 1e-300),
+        "batched_flips": int(flips.item()),
+        "batched_status": int(status.item()),
+        "reaches_plain_best": e64 >= e_plain * (1.0 - 1e-5),
+        "speedup": t_plain / t_batched,
+    }
+
+
 def make_graph():
     from pyqrackising_b200 import workloads as wl
 
@@ -236,8 +300,9 @@ def make_batch(seed):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--no-ttb", action="store_true", help="skip the SK n=8192 time-to-best leg")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     args = ap.parse_args()
 
@@ -291,6 +356,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local_rank) as clocks:
+        clocks.wait_first()
         wall0 = time.perf_counter()
         for i in range(args.steps):
             flush.fill_(i & 0xFF)
@@ -366,19 +432,27 @@ def main():
             "bound": "tensor",
             "achieved": achieved,
             "peak": int8_peak,
-            "unit": "TOPS",
+            "unit": "TFLOP/s",
             "frac": achieved / int8_peak,
-            "traffic": None,
+            "ops_note": "int8 multiply-adds counted as 2 ops (TOPS)",
+            # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this
+            # workload (profiles/score_tc_kernel_er2048_b65536.md)
+            "traffic": 195.9e6,
+            "traffic_unit": "bytes per launch (ncu)",
+            "algorithmic_bytes_per_launch": float(BATCH * N_NODES + N_NODES * N_NODES + BATCH * N_NODES // 8),
             "peak_basis": f"int8 dense = 2 x bf16 dense ({src} bf16 {bf16} TFLOP/s)",
             "kernel": "score_tc_kernel<int8> (tcgen05 GEMM + row-dot epilogue), CUDA events around the launch",
             "kernel_ms": kernel_ms,
             "algorithmic_ops_per_launch": ops,
         },
-        "gpu_launches": 4 * args.steps,
+        # per step: expand_pm1_kernel + score_tc_kernel (the L2 flush is torch's fill)
+        "gpu_launches": 2 * args.steps,
         "wall_s_timed_loop": wall,
     }
     if rank == 0:
         line["clocks"] = clocks.summary()
+        if world == 1 and not args.no_ttb:
+            line["time_to_best"] = time_to_best()
         if world == 1:
             try:
                 line["cpu_baseline"] = cpu_baseline(W, make_batch(0))

@@ -377,10 +377,27 @@ extern "C" pqi_status pqi_cluster_ascent(const void* graphs, int num_graphs,
     PQI_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (cluster_size > 8)
       PQI_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    // as many clusters as fit at once; each loops over tasks
-    cfg.gridDim = dim3(cluster_size);
+    // as many clusters as fit at once; each loops over tasks (the occupancy
+    // query is cached per kernel and launch shape: it is slow on first use)
+    struct FitEntry {
+      const void* k;
+      size_t smem;
+      int T, cs, dev, fit;
+    };
+    static FitEntry cache[32];
+    static int cached = 0;
+    int dev = 0;
+    PQI_TRY(cudaGetDevice(&dev));
     int fit = 0;
-    PQI_TRY(cudaOccupancyMaxActiveClusters(&fit, kern, &cfg));
+    for (int e = 0; e < cached; ++e)
+      if (cache[e].k == (const void*)kern && cache[e].smem == smem && cache[e].T == T &&
+          cache[e].cs == cluster_size && cache[e].dev == dev)
+        fit = cache[e].fit;
+    if (fit == 0) {
+      cfg.gridDim = dim3(cluster_size);
+      PQI_TRY(cudaOccupancyMaxActiveClusters(&fit, kern, &cfg));
+      if (fit > 0 && cached < 32) cache[cached++] = {(const void*)kern, smem, T, cluster_size, dev, fit};
+    }
     if (fit < 1) {
       set_error_text("cluster ascent: the cluster does not fit on the device");
       return PQI_EINVAL;
