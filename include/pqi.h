@@ -313,6 +313,22 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
                             unsigned long long* flips_total, int* status, void* stream);
 
 /*
+ * pqi_batch_search with one warp per task instead of one CTA: the same search,
+ * selection rule, kick stream, outputs and status, for graphs with
+ * max_n <= 1024. Fields and bits live in registers (no shared memory, no
+ * block barrier), so many more tasks are in flight per SM. warps_per_sm caps
+ * the resident warps per SM (0 = as many as fit). No reference counterpart
+ * (batched form of spin_glass_solver.py:603-717).
+ */
+pqi_status pqi_batch_search_warp(const void* graphs, int num_graphs, const int* task_graph,
+                                 const uint32_t* init_states, int words_pitch, int tasks,
+                                 int max_n, int kind, int is_spin_glass, int rounds, int kick,
+                                 int flip_budget, uint64_t seed, const double* kick_cdf,
+                                 const long long* cdf_offset, uint32_t* best_states,
+                                 double* best_values, unsigned long long* flips_total,
+                                 int* status, int warps_per_sm, void* stream);
+
+/*
  * Steepest single-flip ascent (rounds = 0 of pqi_batch_search: same selection
  * rule, same trajectory, same outputs and status) with one thread-block
  * cluster of cluster_size CTAs (2, 4, 8 or 16) per task: the task's nodes are

@@ -75,14 +75,33 @@ class BatchedSearch:
 
     def run(self, task_graph, init_words: torch.Tensor, is_spin_glass: bool, rounds: int = 0, kick: int = 4,
             seed: int = 0, kick_cdf: torch.Tensor | None = None, cdf_offset: torch.Tensor | None = None,
-            flip_budget: int | None = None):
-        tg = torch.as_tensor(np.asarray(task_graph, dtype=np.int32)).to(self.device)
+            flip_budget: int | None = None, variant: str = "cta", warps_per_sm: int = 0, out=None):
+        """Iterated local search of every task. variant: "cta" (one CTA per
+        task, any n) or "warp" (one warp per task, max_n <= 1024); both give
+        the same results. `out` = (best_states, best_values, flips, status)
+        device buffers to fill (for CUDA-graph capture); flips and status are
+        accumulated into, so zero them between uses."""
+        tg = task_graph if torch.is_tensor(task_graph) else torch.as_tensor(np.asarray(task_graph, dtype=np.int32)).to(self.device)
         tasks = int(tg.numel())
-        best_states = torch.zeros(tasks * self.pitch, dtype=torch.int32, device=self.device)
-        best_values = torch.empty(tasks, dtype=torch.float64, device=self.device)
-        flips = torch.zeros(1, dtype=torch.int64, device=self.device)
-        status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        if out is None:
+            best_states = torch.zeros(tasks * self.pitch, dtype=torch.int32, device=self.device)
+            best_values = torch.empty(tasks, dtype=torch.float64, device=self.device)
+            flips = torch.zeros(1, dtype=torch.int64, device=self.device)
+            status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        else:
+            best_states, best_values, flips, status = out
         budget = int(flip_budget) if flip_budget is not None else 4 * self.max_n + 64
+        if variant == "warp":
+            _lib.call(
+                "pqi_batch_search_warp", D._ptr(self.desc), len(self.graphs), D._ptr(tg), D._ptr(init_words),
+                self.pitch, tasks, self.max_n, int(self.kind), int(bool(is_spin_glass)), int(rounds), int(kick),
+                budget, ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), D._ptr(kick_cdf), D._ptr(cdf_offset),
+                D._ptr(best_states), D._ptr(best_values), D._ptr(flips), D._ptr(status), int(warps_per_sm),
+                D.stream_ptr(self.stream),
+            )
+            return best_values, best_states.view(tasks, self.pitch), flips, status
+        if variant != "cta":
+            raise ValueError("variant must be 'cta' or 'warp'")
         _lib.call(
             "pqi_batch_search",
             D._ptr(self.desc),
@@ -147,3 +166,142 @@ class BatchedSearch:
             bits = np.unpackbits(w[t].view(np.uint8), bitorder="little")[: int(self.n[g])].astype(np.bool_)
             out.append(bits)
         return out
+
+
+class BatchedSolver:
+    """Many graphs of mixed weight kinds, many starting states per graph.
+
+    Graphs are grouped by weight kind (int8 vs float32 launches). For each
+    group a small autotuner times the kernel forms (one CTA per task, or one
+    warp per task with an occupancy cap) on a sample of tasks and keeps the
+    fastest; `capture()` then records every launch of a step in one CUDA
+    graph, so a step is one graph replay. Results are the best value and state
+    per graph over its seeds (reduced on the device).
+    """
+
+    FORMS = (("cta", 0), ("warp", 0), ("warp", 16), ("warp", 8))
+
+    def __init__(self, graphs: list[D.DeviceGraph], seeds_per_graph: int, is_spin_glass: bool,
+                 rounds: int = 0, kick: int = 8, seed: int = 0, stream=None):
+        if seeds_per_graph < 1:
+            raise ValueError("seeds_per_graph must be >= 1")
+        self.graphs = graphs
+        self.S = int(seeds_per_graph)
+        self.spin = bool(is_spin_glass)
+        self.rounds, self.kick, self.seed = int(rounds), int(kick), int(seed)
+        self.stream = stream
+        self.groups = []
+        for kind in sorted({g.w.kind for g in graphs}):
+            idx = [i for i, g in enumerate(graphs) if g.w.kind == kind]
+            bs = BatchedSearch([graphs[i] for i in idx], stream=stream)
+            tg = np.repeat(np.arange(len(idx), dtype=np.int32), self.S)
+            self.groups.append({
+                "kind": kind, "index": idx, "bs": bs,
+                "tg": torch.from_numpy(tg).to(bs.device),
+                "form": ("cta", 0),
+            })
+        self.graph = None
+        self.tuning = {}
+
+    def autotune(self, sample_tasks: int | None = None, reps: int = 2):
+        """Time each kernel form on every group's tasks (or on a sample of
+        them, graphs taken evenly across the group) and keep the fastest.
+        The full task set is the default: a persistent launch's speed depends
+        on how many tasks each resident CTA or warp gets, which a small sample
+        does not show."""
+        for grp in self.groups:
+            bs = grp["bs"]
+            tasks = int(grp["tg"].numel())
+            count = tasks if sample_tasks is None else min(int(sample_tasks), tasks)
+            take = np.linspace(0, tasks - 1, num=count).astype(np.int64)
+            tg = grp["tg"][torch.from_numpy(take).to(bs.device)].contiguous()
+            words = bs.random_states(tg.cpu().numpy(), seed=self.seed + 99)
+            times = {}
+            for form, wps in self.FORMS:
+                if form == "warp" and bs.max_n > 1024:
+                    continue
+                best = float("inf")
+                for _ in range(reps + 1):  # first run warms the launch
+                    s0 = torch.cuda.Event(enable_timing=True)
+                    s1 = torch.cuda.Event(enable_timing=True)
+                    s0.record()
+                    bs.run(tg, words, self.spin, rounds=self.rounds, kick=self.kick, seed=self.seed,
+                           variant=form, warps_per_sm=wps)
+                    s1.record()
+                    s1.synchronize()
+                    best = min(best, s0.elapsed_time(s1))
+                times[(form, wps)] = best
+            grp["form"] = min(times, key=times.get)
+            self.tuning[int(grp["kind"])] = {f"{k[0]}/{k[1]}": v for k, v in times.items()}
+        return self.tuning
+
+    def _buffers(self):
+        for grp in self.groups:
+            bs = grp["bs"]
+            tasks = int(grp["tg"].numel())
+            grp["init"] = torch.zeros(tasks, bs.pitch, dtype=torch.int32, device=bs.device)
+            grp["out"] = (
+                torch.zeros(tasks * bs.pitch, dtype=torch.int32, device=bs.device),
+                torch.empty(tasks, dtype=torch.float64, device=bs.device),
+                torch.zeros(1, dtype=torch.int64, device=bs.device),
+                torch.zeros(1, dtype=torch.int32, device=bs.device),
+            )
+
+    def set_starts(self, seed: int):
+        """Fresh uniform random starting states for every task (device side)."""
+        if "init" not in self.groups[0]:
+            self._buffers()
+        for grp in self.groups:
+            grp["init"].copy_(grp["bs"].random_states(grp["tg"].cpu().numpy(), seed=seed))
+
+    def _launch_all(self):
+        for grp in self.groups:
+            bs = grp["bs"]
+            st, bv, fl, stt = grp["out"]
+            fl.zero_()
+            stt.zero_()
+            form, wps = grp["form"]
+            bs.run(grp["tg"], grp["init"], self.spin, rounds=self.rounds, kick=self.kick, seed=self.seed,
+                   variant=form, warps_per_sm=wps, out=grp["out"])
+
+    def capture(self):
+        """Record one step (every group's launch) in a CUDA graph."""
+        if "init" not in self.groups[0]:
+            self._buffers()
+        self._launch_all()  # warm: function attributes, occupancy queries
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._launch_all()
+        self.graph = g
+        return g
+
+    def step(self):
+        """One step: replay the captured graph (or launch directly)."""
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._launch_all()
+
+    def results(self):
+        """(best value per graph [G] float64, best state words per graph, flips, status)."""
+        G = len(self.graphs)
+        dev = self.groups[0]["bs"].device
+        values = torch.empty(G, dtype=torch.float64, device=dev)
+        states = [None] * G
+        flips = 0
+        status = 0
+        for grp in self.groups:
+            bs = grp["bs"]
+            st, bv, fl, stt = grp["out"]
+            v = bv.view(-1, self.S)
+            best, arg = torch.max(v, dim=1)  # first maximum: the lowest seed on ties
+            idx = torch.as_tensor(grp["index"], device=dev)
+            values[idx] = best
+            words = st.view(-1, self.S, bs.pitch)
+            pick = words[torch.arange(v.shape[0], device=dev), arg]
+            for j, gi in enumerate(grp["index"]):
+                states[gi] = pick[j]
+            flips += int(fl.item())
+            status = max(status, int(stt.item()))
+        return values, states, flips, status

@@ -139,3 +139,77 @@ def test_cluster_ascent_flip_budget_reports_timeout():
     assert torch.equal(bbest, best)
     assert int(flips.item()) == int(bflips.item()) == 10
     assert torch.allclose(vals, bvals, rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("kind", ["int", "float"])
+def test_warp_form_matches_cta_form(kind):
+    """One warp per task gives the CTA form's best states, values and flip
+    counts, with rounds of uniform and proposal-drawn kicks, on uneven sizes
+    that cover every register-group count (n <= 128, 256, 512, 1024)."""
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    Ws = _graphs(kind, [40, 100, 129, 250, 300, 513, 777, 1024], seed=11)
+    bs = BatchedSearch([DeviceGraph(W) for W in Ws])
+    task_graph = [g for g in range(len(Ws)) for _ in range(5)]
+    words = bs.random_states(task_graph, seed=9)
+    # a proposal distribution per graph (normalised cumulative sums)
+    rng = np.random.default_rng(4)
+    cdfs, offs, off = [], [], 0
+    for W in Ws:
+        p = rng.random(W.shape[0]) + 0.05
+        c = np.cumsum(p / p.sum())
+        c[-1] = 1.0
+        cdfs.append(c)
+        offs.append(off)
+        off += len(c)
+    cdf = torch.from_numpy(np.concatenate(cdfs)).cuda()
+    off_t = torch.tensor(offs, dtype=torch.int64).cuda()
+    for spin in (0, 1):
+        for rounds, kick, use_cdf in ((0, 0, False), (3, 8, False), (2, 5, True)):
+            kw = dict(rounds=rounds, kick=kick, seed=123, kick_cdf=cdf if use_cdf else None,
+                      cdf_offset=off_t if use_cdf else None)
+            v1, b1, f1, s1 = bs.run(task_graph, words, spin, variant="cta", **kw)
+            v2, b2, f2, s2 = bs.run(task_graph, words, spin, variant="warp", **kw)
+            assert int(s1.item()) == int(s2.item()) == 0
+            assert torch.equal(b1, b2), (spin, rounds, kick, use_cdf)
+            assert int(f1.item()) == int(f2.item())
+            if kind == "int":
+                assert torch.equal(v1, v2)
+            else:
+                assert torch.allclose(v1, v2, rtol=1e-12, atol=1e-9)
+
+
+def test_batched_solver_mixed_kinds_graph_capture(oracle_mod):
+    """Mixed int8/float graphs, several seeds each: autotuned forms, one CUDA
+    graph per step; per-graph results equal the best of a direct run and are
+    local optima whose values match float64 re-scoring."""
+    from pyqrackising_b200 import workloads as wl
+    from pyqrackising_b200.batch import BatchedSearch, BatchedSolver
+    from pyqrackising_b200.device import DeviceGraph
+
+    O = oracle_mod
+    Ws = wl.batched_uneven(8, lo=64, hi=300, seed=3)
+    dgs = [DeviceGraph(W) for W in Ws]
+    solver = BatchedSolver(dgs, seeds_per_graph=6, is_spin_glass=True, rounds=2, kick=6, seed=5)
+    tuning = solver.autotune(sample_tasks=24, reps=1)
+    assert tuning and all(len(v) >= 2 for v in tuning.values())
+    solver.set_starts(seed=17)
+    solver.capture()
+    solver.step()
+    torch.cuda.synchronize()
+    values, states, flips, status = solver.results()
+    assert status == 0 and flips > 0
+    for gi, W in enumerate(Ws):
+        n = W.shape[0]
+        bits = np.unpackbits(states[gi].cpu().numpy().view(np.uint8), bitorder="little")[:n].astype(bool)
+        assert float(values[gi]) == pytest.approx(O.compute_energy(bits, W), rel=1e-9, abs=1e-6)
+        x = np.where(bits, 1.0, -1.0)
+        Wd = W.astype(np.float64).copy()
+        np.fill_diagonal(Wd, 0.0)
+        assert np.all(x * (Wd @ x) <= 1e-6 * np.abs(Wd).sum(axis=1).max())  # local optimum
+    # the replay equals a direct run of the same group
+    grp = solver.groups[0]
+    form, wps = grp["form"]
+    v2, _, _, _ = grp["bs"].run(grp["tg"], grp["init"], True, rounds=2, kick=6, seed=5, variant=form, warps_per_sm=wps)
+    assert torch.allclose(v2, grp["out"][1], rtol=0, atol=0)
