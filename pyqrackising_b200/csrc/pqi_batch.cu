@@ -45,6 +45,14 @@ __device__ __forceinline__ double bunif(uint64_t seed, uint64_t a, uint64_t b) {
   return (double)(h >> 11) * (1.0 / 9007199254740992.0);
 }
 
+// Shared-memory position of node v's field (256-thread CTAs): node
+// v = 4 t + 1024 j + i (thread t's group j, lane i of the group) sits at
+// (4 j + i) * 256 + t, so a warp's accesses in the flip pass are contiguous.
+// Holds ceil(n / 1024) * 1024 entries.
+__device__ __forceinline__ int fpos(int v) {
+  return (((v >> 10) << 2) + (v & 3)) * 256 + ((v >> 2) & 255);
+}
+
 template <typename WT, typename GT>
 struct TaskCtx {
   const WT* W;
@@ -53,83 +61,105 @@ struct TaskCtx {
   uint32_t* bits;
 };
 
+__device__ __forceinline__ unsigned long long bkey(float gv, int v, int xv) {
+  return ((unsigned long long)ord_f32(gv) << 32) |
+         (unsigned long long)(((0x3FFFFFFFu - (uint32_t)v) << 1) | (uint32_t)xv);
+}
+
+__device__ __forceinline__ unsigned long long bmax_key(unsigned long long key) {
+  const uint32_t hi = __reduce_max_sync(0xFFFFFFFFu, (uint32_t)(key >> 32));
+  const uint32_t lo =
+      __reduce_max_sync(0xFFFFFFFFu, ((uint32_t)(key >> 32) == hi) ? (uint32_t)key : 0u);
+  return ((unsigned long long)hi << 32) | lo;
+}
+
 // The task keeps the local field y = W x (x = 2s - 1) instead of the gains:
 // the gain of node v is g_v = x_v y_v, and flipping node k changes every
 // field by y_v -= 2 x_k W_kv (W's prepared copy has a zero diagonal, so y_k is
-// unchanged). One fused pass per flip: each thread loads its whole slice of
-// row k first (all loads in flight at once), applies the update, and folds
-// the new gains into a (float gain, lowest node) block argmax. Thread 0
-// toggles bit k between the reduction's two barriers, when every thread has
-// finished reading the bits and before anyone reads them again. Two barriers
-// per flip. k < 0: no flip, only the argmax.
+// unchanged). One fused pass per flip, one CTA barrier: each thread owns
+// groups of four consecutive nodes v = 4 t + 1024 j + i, loads CH groups of
+// row k at once (float4 / char4), updates their fields, toggles bit k if it
+// owns k (the only writer of that bit; the other nodes of the word are read
+// by their own threads only), and folds the new gains into a key (float gain,
+// then the lowest node, then the node's bit). Warp maxima go to a slot array
+// chosen by the pass parity; after the barrier every warp reduces the slots
+// itself, so the next pass starts without a second barrier (a warp can be at
+// most one pass ahead of another, which writes the other slot array).
+// k < 0: no flip, only the selection. Returns the key and the exact gain.
 template <typename WT, typename GT, int CH>
-__device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k, float* red_v,
-                                                int* red_i, float* out_v, int* out_i) {
-  float bv = -INFINITY;
-  int bi = 0x7FFFFFFF;
+__device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k, int xk,
+                                                unsigned long long (*red_key)[8],
+                                                double (*red_g)[8], int par,
+                                                unsigned long long* out_key, double* out_g) {
   const int n = c.n;
-  const GT coef = (k >= 0) ? (((c.bits[k >> 5] >> (k & 31)) & 1) ? (GT)-2 : (GT)2) : (GT)0;
+  const GT coef = (k >= 0) ? (xk ? (GT)-2 : (GT)2) : (GT)0;
   const WT* __restrict__ row = c.W + (size_t)(k >= 0 ? k : 0) * c.ld;
-  for (int base = threadIdx.x; base < n; base += CH * blockDim.x) {
-    WT w[CH];
+  float bv = -INFINITY;
+  int bi = -1, bx = 0;
+  double bg = 0.0;
+  constexpr int stride = 1024;  // 4 nodes x 256 threads
+  for (int base = 4 * threadIdx.x; base < n; base += CH * stride) {
+    WT w[4 * CH];
     if (k >= 0) {
 #pragma unroll
-      for (int i = 0; i < CH; ++i) {
-        const int v = base + i * blockDim.x;
-        w[i] = v < n ? __ldg(row + v) : (WT)0;
-      }
-    }
+      for (int j = 0; j < CH; ++j) {
+        const int v = base + j * stride;
+        if (v + 3 < n) {
+          if constexpr (sizeof(WT) == 4) {
+            const float4 t = __ldg(reinterpret_cast<const float4*>(row + v));
+            w[4 * j] = t.x; w[4 * j + 1] = t.y; w[4 * j + 2] = t.z; w[4 * j + 3] = t.w;
+          } else {
+            const char4 t = __ldg(reinterpret_cast<const char4*>(row + v));
+            w[4 * j] = t.x; w[4 * j + 1] = t.y; w[4 * j + 2] = t.z; w[4 * j + 3] = t.w;
+          }
+        } else {
 #pragma unroll
-    for (int i = 0; i < CH; ++i) {
-      const int v = base + i * blockDim.x;
-      if (v < n) {
-        GT y = c.g[v];
-        if (k >= 0) {
-          y += coef * (GT)w[i];
-          c.g[v] = y;
-        }
-        // node k's bit is toggled only after this pass: use its new value here
-        const bool xv = (((c.bits[v >> 5] >> (v & 31)) & 1) != 0) != (v == k);
-        const float gv = (float)(xv ? y : -y);
-        if (gv > bv) {  // v ascends within a thread: strict '>' keeps the lowest node
-          bv = gv;
-          bi = v;
+          for (int i = 0; i < 4; ++i) w[4 * j + i] = (v + i < n) ? __ldg(row + v + i) : (WT)0;
         }
       }
     }
-  }
-  // warp then block argmax: larger gain, then lower node
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
-    const int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
-    if (ov > bv || (ov == bv && oi < bi)) {
-      bv = ov;
-      bi = oi;
+    for (int j = 0; j < CH; ++j) {
+      const int v0 = base + j * stride;
+      if (v0 < n) {
+        if (k >= v0 && k < v0 + 4) c.bits[k >> 5] ^= 1u << (k & 31);
+        const uint32_t word = c.bits[v0 >> 5];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int v = v0 + i;
+          if (v < n) {
+            GT y = c.g[fpos(v)];
+            if (k >= 0) {
+              y += coef * (GT)w[4 * j + i];
+              c.g[fpos(v)] = y;
+            }
+            const int xv = (word >> (v & 31)) & 1;
+            const double g = xv ? (double)y : -(double)y;
+            const float gv = (float)g;
+            if (gv > bv) {  // v ascends within a thread: strict '>' keeps the lowest node
+              bv = gv;
+              bi = v;
+              bg = g;
+              bx = xv;
+            }
+          }
+        }
+      }
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nwarps = (blockDim.x + 31) >> 5;
-  if (lane == 0) {
-    red_v[warp] = bv;
-    red_i[warp] = bi;
-  }
+  const unsigned long long key = bi >= 0 ? bkey(bv, bi, bx) : 0ull;
+  const unsigned long long wk = bmax_key(key);
+  if (lane == 0) red_key[par][warp] = wk;
+  if (key != 0ull && key == wk) red_g[par][warp] = bg;
   __syncthreads();
-  if (threadIdx.x == 0 && k >= 0) c.bits[k >> 5] ^= 1u << (k & 31);
-  bv = lane < nwarps ? red_v[lane] : -INFINITY;
-  bi = lane < nwarps ? red_i[lane] : 0x7FFFFFFF;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
-    const int oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
-    if (ov > bv || (ov == bv && oi < bi)) {
-      bv = ov;
-      bi = oi;
-    }
-  }
-  __syncthreads();
-  *out_v = bv;
-  *out_i = bi;
+  const int nwarps = blockDim.x >> 5;
+  const unsigned long long sk = lane < nwarps ? red_key[par][lane] : 0ull;
+  const double sg = lane < nwarps ? red_g[par][lane] : 0.0;
+  const unsigned long long gk = bmax_key(sk);
+  const uint32_t src = __ballot_sync(0xFFFFFFFFu, sk == gk && gk != 0ull);
+  *out_g = __shfl_sync(0xFFFFFFFFu, sg, src ? __ffs(src) - 1 : 0);
+  *out_key = gk;
 }
 
 template <typename WT, int CH>
@@ -143,9 +173,8 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
   typedef typename std::conditional<sizeof(WT) == 1, int, double>::type GT;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[32];
-  __shared__ float red_v[32];
-  __shared__ int red_i[32];
-  __shared__ int s_pick;
+  __shared__ unsigned long long red_key[2][8];
+  __shared__ double red_g[2][8];
   for (int task = blockIdx.x; task < tasks; task += gridDim.x) {
     const BatchGraph G = graphs[task_graph[task]];
     const int n = G.n, n32 = (n + 31) >> 5;
@@ -169,14 +198,14 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
           acc += ((c.bits[v >> 5] >> (v & 31)) & 1) ? w : -w;
         }
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
-        if (lane == 0) c.g[k] = acc;  // local field y_k
+        if (lane == 0) c.g[fpos(k)] = acc;  // local field y_k
       }
     }
     __syncthreads();
     // q = x^T W x = sum_k x_k y_k; value from q
     double part = 0.0;
     for (int v = threadIdx.x; v < n; v += blockDim.x)
-      part += ((c.bits[v >> 5] >> (v & 31)) & 1) ? (double)c.g[v] : -(double)c.g[v];
+      part += ((c.bits[v >> 5] >> (v & 31)) & 1) ? (double)c.g[fpos(v)] : -(double)c.g[fpos(v)];
     for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xFFFFFFFFu, part, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
     __syncthreads();
@@ -188,22 +217,23 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
     double best = -INFINITY;
     unsigned long long nflips = 0;
     int timeout = 0;
-    float gv;
-    int k;
-    flip_and_select<WT, GT, CH>(c, -1, red_v, red_i, &gv, &k);
+    unsigned long long key;
+    double gk;
+    int par = 0;
+    flip_and_select<WT, GT, CH>(c, -1, 0, red_key, red_g, par, &key, &gk);
+    par ^= 1;
     for (int r = 0; r <= rounds; ++r) {
       // steepest ascent: flip the best node while its gain is positive
       for (int f = 0;; ++f) {
-        if (!(gv > 0.0f)) break;
+        if (key == 0ull || !(unord_f32((uint32_t)(key >> 32)) > 0.0f)) break;
         if (f >= flip_budget) {
           timeout = 1;
           break;
         }
-        // exact gain before the flip: x_k y_k (bits and fields are stable here)
-        const double gk = ((c.bits[k >> 5] >> (k & 31)) & 1) ? (double)c.g[k] : -(double)c.g[k];
-        __syncthreads();
-        val += scale * gk;
-        flip_and_select<WT, GT, CH>(c, k, red_v, red_i, &gv, &k);
+        const int k = (int)(0x3FFFFFFFu - (((uint32_t)key) >> 1));
+        val += scale * gk;  // exact gain of k before the flip
+        flip_and_select<WT, GT, CH>(c, k, (int)(key & 1ull), red_key, red_g, par, &key, &gk);
+        par ^= 1;
         ++nflips;
       }
       if (val > best) {
@@ -211,36 +241,33 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
         for (int w = threadIdx.x; w < n32; w += blockDim.x) best_bits[w] = c.bits[w];
       }
       if (r == rounds) break;
-      // kick: forced flips
+      // kick: forced flips; every thread draws the same node
       for (int j = 0; j < kick; ++j) {
-        if (threadIdx.x == 0) {
-          int pick;
-          const double u = bunif(seed, (uint64_t)task * 1315423911ull + r, (uint64_t)j);
-          if (kick_cdf) {
-            // first node whose cumulative proposal mass exceeds u
-            const double* cdf = kick_cdf + cdf_offset[task_graph[task]];
-            int lo = 0, hi = n - 1;
-            while (lo < hi) {
-              const int mid = (lo + hi) >> 1;
-              if (cdf[mid] > u) {
-                hi = mid;
-              } else {
-                lo = mid + 1;
-              }
+        int pick;
+        const double u = bunif(seed, (uint64_t)task * 1315423911ull + r, (uint64_t)j);
+        if (kick_cdf) {
+          // first node whose cumulative proposal mass exceeds u
+          const double* cdf = kick_cdf + cdf_offset[task_graph[task]];
+          int lo = 0, hi = n - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (cdf[mid] > u) {
+              hi = mid;
+            } else {
+              lo = mid + 1;
             }
-            pick = lo;
-          } else {
-            pick = (int)(u * n);
-            if (pick >= n) pick = n - 1;
           }
-          s_pick = pick;
+          pick = lo;
+        } else {
+          pick = (int)(u * n);
+          if (pick >= n) pick = n - 1;
         }
-        __syncthreads();
-        const int kk = s_pick;
-        const double gk = ((c.bits[kk >> 5] >> (kk & 31)) & 1) ? (double)c.g[kk] : -(double)c.g[kk];
-        __syncthreads();
-        val += scale * gk;
-        flip_and_select<WT, GT, CH>(c, kk, red_v, red_i, &gv, &k);
+        const int xp = (c.bits[pick >> 5] >> (pick & 31)) & 1;
+        const double gp = xp ? (double)c.g[fpos(pick)] : -(double)c.g[fpos(pick)];
+        __syncthreads();  // everyone has read bit and field before the owner changes them
+        val += scale * gp;
+        flip_and_select<WT, GT, CH>(c, pick, xp, red_key, red_g, par, &key, &gk);
+        par ^= 1;
         ++nflips;
       }
     }
@@ -261,18 +288,6 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
 // registers, and reads its four weights of row k with one vector load per i
 // (a warp reads 512 B of a float row, 128 B of an int8 row, per i). A flip is
 // NG loads, 4 NG updates and a two-step 32-bit redux argmax: no barrier.
-
-__device__ __forceinline__ unsigned long long wkey(float gv, int v, int xv) {
-  return ((unsigned long long)ord_f32(gv) << 32) |
-         (unsigned long long)(((0x3FFFFFFFu - (uint32_t)v) << 1) | (uint32_t)xv);
-}
-
-__device__ __forceinline__ unsigned long long wmax_key(unsigned long long key) {
-  const uint32_t hi = __reduce_max_sync(0xFFFFFFFFu, (uint32_t)(key >> 32));
-  const uint32_t lo =
-      __reduce_max_sync(0xFFFFFFFFu, ((uint32_t)(key >> 32) == hi) ? (uint32_t)key : 0u);
-  return ((unsigned long long)hi << 32) | lo;
-}
 
 // One pass of the warp form: apply flip k (coef = -2 x_k; k < 0: none) to the
 // lane's fields and bits, then the warp's best key (float gain, lowest node)
@@ -325,8 +340,8 @@ __device__ __forceinline__ void warp_pass(const WT* __restrict__ W, int ld, int 
       bg = bx ? (double)y[e] : -(double)y[e];
     }
   const unsigned long long key =
-      bs >= 0 ? wkey(bv, 128 * (bs >> 2) + 4 * lane + (bs & 3), bx) : 0ull;
-  const unsigned long long wk = wmax_key(key);
+      bs >= 0 ? bkey(bv, 128 * (bs >> 2) + 4 * lane + (bs & 3), bx) : 0ull;
+  const unsigned long long wk = bmax_key(key);
   const uint32_t src = __ballot_sync(0xFFFFFFFFu, key == wk && wk != 0ull);
   *gk = __shfl_sync(0xFFFFFFFFu, bg, src ? __ffs(src) - 1 : 0);
   *gkey = wk;
@@ -497,7 +512,7 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
   cudaStream_t s = as_stream(stream);
   const bool i8 = kind == PQI_W_I8;
   const size_t smem = (((size_t)((max_n + 31) >> 5) * 4 + 15) & ~size_t(15)) +
-                      (size_t)max_n * (i8 ? sizeof(int) : sizeof(double));
+                      (size_t)((max_n + 1023) / 1024 * 1024) * (i8 ? sizeof(int) : sizeof(double));
   PQI_CHECK_ARG(smem <= 200 * 1024);
   static int num_sms = 0;
   if (!num_sms) {
@@ -505,34 +520,39 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev);
   }
-  const int per_sm = std::max(1, std::min(8, (int)((220 * 1024) / (smem + 2048))));
-  const int grid = std::max(1, std::min(tasks, num_sms * per_sm));
+  // persistent grid: exactly the CTAs that are resident at once
+  int per_sm = 1;
   const BatchGraph* gd = static_cast<const BatchGraph*>(graphs);
-  // row loads per thread in chunks of CH (8 for n <= 2048, else 16; three CTAs
-  // per SM cap the registers)
+  // row loads per thread: groups of four nodes, CH groups in flight per chunk
+  // (the whole row for n <= 4 * 256 * CH). CH = 4 keeps three CTAs per SM
+  // within the register file (8 groups spill at that occupancy and run slower
+  // on SK n = 8192 than two chunks of 4).
 #define PQI_BATCH_LAUNCH(WT_, CH_)                                                              \
   do {                                                                                         \
     PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_>,                               \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
     PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_>,                               \
                                  cudaFuncAttributePreferredSharedMemoryCarveout, 100));        \
+    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel<WT_, CH_>, \
+                                                          256, smem));                         \
+    const int grid = std::max(1, std::min(tasks, num_sms * std::max(1, per_sm)));             \
     batch_search_kernel<WT_, CH_><<<grid, 256, smem, s>>>(                                     \
         gd, task_graph, init_states, words_pitch, tasks, is_spin_glass, rounds, kick,          \
         flip_budget, seed, kick_cdf, cdf_offset, best_states, best_values, flips_total,        \
         status);                                                                               \
   } while (0)
-  const int per_thread = (max_n + 255) / 256;
+  const int groups = (max_n + 1023) / 1024;  // groups of four per thread
   if (i8) {
-    if (per_thread <= 8) {
-      PQI_BATCH_LAUNCH(int8_t, 8);
+    if (groups <= 2) {
+      PQI_BATCH_LAUNCH(int8_t, 2);
     } else {
-      PQI_BATCH_LAUNCH(int8_t, 16);
+      PQI_BATCH_LAUNCH(int8_t, 4);
     }
   } else {
-    if (per_thread <= 8) {
-      PQI_BATCH_LAUNCH(float, 8);
+    if (groups <= 2) {
+      PQI_BATCH_LAUNCH(float, 2);
     } else {
-      PQI_BATCH_LAUNCH(float, 16);
+      PQI_BATCH_LAUNCH(float, 4);
     }
   }
 #undef PQI_BATCH_LAUNCH
