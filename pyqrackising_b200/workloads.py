@@ -103,3 +103,40 @@ def random_bits(n: int, seed: int, batch: int | None = None) -> np.ndarray:
     rng = np.random.default_rng(seed)
     shape = (n,) if batch is None else (batch, n)
     return rng.random(shape) < 0.5
+
+
+def regular_pm1_np(n: int, seed: int, degree: int = 3, max_tries: int = 1000) -> np.ndarray:
+    """Random `degree`-regular graph with a +-1 weight per edge, drawn with the
+    pairing model in numpy (shuffle n * degree stubs, pair neighbours, retry
+    while a pair is a loop or repeats an edge): uniform over simple regular
+    graphs, and fast enough to stream thousands of training graphs."""
+    if (n * degree) % 2:
+        raise ValueError("n * degree must be even")
+    rng = np.random.default_rng(seed)
+    stubs = np.repeat(np.arange(n, dtype=np.int64), degree)
+    for _ in range(max_tries):
+        rng.shuffle(stubs)
+        a, b = stubs[0::2], stubs[1::2]
+        if np.any(a == b):
+            continue
+        lo, hi = np.minimum(a, b), np.maximum(a, b)
+        key = lo * n + hi
+        if np.unique(key).size != key.size:
+            continue
+        W = np.zeros((n, n), dtype=np.float32)
+        s = rng.choice(np.array([-1.0, 1.0], dtype=np.float32), size=key.size)
+        W[lo, hi] = s
+        W[hi, lo] = s
+        return W
+    raise RuntimeError("no simple regular graph drawn")
+
+
+def proposal_training_graph(i: int, seed: int = 0, lo: int = 128, hi: int = 2048) -> np.ndarray:
+    """The i-th graph of the proposal-network training stream: n ~ U[lo, hi];
+    even i: 3-regular +-1, odd i: G(n, 0.05) with N(0, 1) weights."""
+    rng = np.random.default_rng([seed, i])
+    n = int(rng.integers(lo, hi + 1))
+    s = int(rng.integers(1 << 30))
+    if i % 2 == 0:
+        return regular_pm1_np(n + (n % 2), seed=s)
+    return gnp_weighted(n, 0.05, seed=s, dist="normal")
