@@ -61,6 +61,25 @@ struct TaskCtx {
   uint32_t* bits;
 };
 
+// Node for a uniform draw u in [0, 1): from the normalised cumulative array
+// `cdf` (first entry above u) or uniformly.
+__device__ __forceinline__ int draw_node(double u, int n, const double* __restrict__ cdf) {
+  if (cdf) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (cdf[mid] > u) {
+        hi = mid;
+      } else {
+        lo = mid + 1;
+      }
+    }
+    return lo;
+  }
+  const int pick = (int)(u * n);
+  return pick >= n ? n - 1 : pick;
+}
+
 __device__ __forceinline__ unsigned long long bkey(float gv, int v, int xv) {
   return ((unsigned long long)ord_f32(gv) << 32) |
          (unsigned long long)(((0x3FFFFFFFu - (uint32_t)v) << 1) | (uint32_t)xv);
@@ -184,6 +203,8 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
     c.ld = G.ld;
     c.bits = reinterpret_cast<uint32_t*>(smem);
     c.g = reinterpret_cast<GT*>(smem + (((size_t)n32 * 4 + 15) & ~size_t(15)));
+    uint32_t* kicked = reinterpret_cast<uint32_t*>(
+        smem + (((size_t)n32 * 4 + 15) & ~size_t(15)) + (size_t)((n + 1023) / 1024 * 1024) * sizeof(GT));
     uint32_t* best_bits = best_states + (size_t)task * words_pitch;
     for (int w = threadIdx.x; w < n32; w += blockDim.x) c.bits[w] = init_states[(size_t)task * words_pitch + w];
     __syncthreads();
@@ -241,30 +262,23 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
         for (int w = threadIdx.x; w < n32; w += blockDim.x) best_bits[w] = c.bits[w];
       }
       if (r == rounds) break;
-      // kick: forced flips; every thread draws the same node
+      // kick: forced flips; every thread draws the same node, without
+      // replacement within the round (a node drawn twice would undo its kick;
+      // after 16 draws that all hit kicked nodes the last draw is taken)
+      for (int w = threadIdx.x; w < n32; w += blockDim.x) kicked[w] = 0u;
+      __syncthreads();
       for (int j = 0; j < kick; ++j) {
-        int pick;
-        const double u = bunif(seed, (uint64_t)task * 1315423911ull + r, (uint64_t)j);
-        if (kick_cdf) {
-          // first node whose cumulative proposal mass exceeds u
-          const double* cdf = kick_cdf + cdf_offset[task_graph[task]];
-          int lo = 0, hi = n - 1;
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (cdf[mid] > u) {
-              hi = mid;
-            } else {
-              lo = mid + 1;
-            }
-          }
-          pick = lo;
-        } else {
-          pick = (int)(u * n);
-          if (pick >= n) pick = n - 1;
+        int pick = 0;
+        for (int attempt = 0; attempt < 16; ++attempt) {
+          const double u =
+              bunif(seed, (uint64_t)task * 1315423911ull + r, (uint64_t)j + ((uint64_t)attempt << 20));
+          pick = draw_node(u, n, kick_cdf ? kick_cdf + cdf_offset[task_graph[task]] : nullptr);
+          if (!((kicked[pick >> 5] >> (pick & 31)) & 1u)) break;
         }
         const int xp = (c.bits[pick >> 5] >> (pick & 31)) & 1;
         const double gp = xp ? (double)c.g[fpos(pick)] : -(double)c.g[fpos(pick)];
-        __syncthreads();  // everyone has read bit and field before the owner changes them
+        __syncthreads();  // everyone has read bit, field and kicked set before they change
+        if (threadIdx.x == 0) kicked[pick >> 5] |= 1u << (pick & 31);
         val += scale * gp;
         flip_and_select<WT, GT, CH>(c, pick, xp, red_key, red_g, par, &key, &gk);
         par ^= 1;
@@ -445,27 +459,19 @@ __global__ void __launch_bounds__(128) warp_search_kernel(
         }
       }
       if (r == rounds) break;
+      // kicks without replacement within the round (as the CTA form): the
+      // kicked set lives in each lane's register, one bit per owned node
+      uint32_t km = 0;
       for (int j = 0; j < kick; ++j) {
-        // every lane draws the same node (same hash, same cumulative array)
-        int pick;
-        const double u = bunif(seed, (uint64_t)task * 1315423911ull + r, (uint64_t)j);
-        if (kick_cdf) {
-          const double* cdf = kick_cdf + cdf_offset[task_graph[task]];
-          int lo = 0, hi = n - 1;
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (cdf[mid] > u) {
-              hi = mid;
-            } else {
-              lo = mid + 1;
-            }
-          }
-          pick = lo;
-        } else {
-          pick = (int)(u * n);
-          if (pick >= n) pick = n - 1;
+        int pick = 0;
+        for (int attempt = 0; attempt < 16; ++attempt) {
+          const double u =
+              bunif(seed, (uint64_t)task * 1315423911ull + r, (uint64_t)j + ((uint64_t)attempt << 20));
+          pick = draw_node(u, n, kick_cdf ? kick_cdf + cdf_offset[task_graph[task]] : nullptr);
+          const int ow = (pick & 127) >> 2, sl = 4 * (pick >> 7) + (pick & 3);
+          if (!((__shfl_sync(0xFFFFFFFFu, km, ow) >> sl) & 1u)) break;
         }
-        // the owner reads the node's bit and exact gain
+        // the owner reads the node's bit and exact gain, and marks it kicked
         const int owner = (pick & 127) >> 2, slot = 4 * (pick >> 7) + (pick & 3);
         double g = 0.0;
         int xv = 0;
@@ -475,6 +481,7 @@ __global__ void __launch_bounds__(128) warp_search_kernel(
             xv = (xm >> e) & 1;
             g = xv ? (double)y[e] : -(double)y[e];
           }
+        if (lane == owner) km |= 1u << slot;
         g = __shfl_sync(0xFFFFFFFFu, g, owner);
         xv = __shfl_sync(0xFFFFFFFFu, xv, owner);
         val += scale * g;
@@ -512,7 +519,8 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
   cudaStream_t s = as_stream(stream);
   const bool i8 = kind == PQI_W_I8;
   const size_t smem = (((size_t)((max_n + 31) >> 5) * 4 + 15) & ~size_t(15)) +
-                      (size_t)((max_n + 1023) / 1024 * 1024) * (i8 ? sizeof(int) : sizeof(double));
+                      (size_t)((max_n + 1023) / 1024 * 1024) * (i8 ? sizeof(int) : sizeof(double)) +
+                      (size_t)((max_n + 31) >> 5) * 4;  // kicked set of the current round
   PQI_CHECK_ARG(smem <= 200 * 1024);
   static int num_sms = 0;
   if (!num_sms) {

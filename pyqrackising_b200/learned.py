@@ -12,8 +12,10 @@ Model (hidden 64, 3 message-passing layers, bf16 weights):
 Training signal: for a local optimum A reached by steepest ascent, the batched
 iterated local search (uniform kicks) finds a better optimum B; the target is
 the uniform distribution over the nodes where A and B differ (the flips that
-led somewhere better). At inference the proposal is the kick distribution of
-the batched search (``BatchedSearch.run(kick_cdf=...)``). The plain search stays
+led somewhere better). At inference each task gets the proposal of its own
+local optimum, flattened by a temperature (``task_proposals``), as the kick
+distribution of the batched search (``BatchedSearch.run(kick_cdf=...)``, one
+graph descriptor per task); kicks are drawn without replacement within a round. The plain search stays
 both the judge (every returned value comes from the search's own exact
 bookkeeping and float64 re-scoring) and the fallback (uniform kicks).
 """
@@ -228,6 +230,30 @@ def _init_params(seed=0):
         else:
             th[o : o + size] = 0.01
     return th
+
+
+def task_proposals(net: "ProposalNet", dg: D.DeviceGraph, words: torch.Tensor, temperature: float = 3.0,
+                   mix: float = 0.0):
+    """One kick distribution per task, from each task's own state: returns
+    (concatenated normalised cumulative arrays, float64; per-task offsets,
+    int64). A proposal p is flattened by the temperature (p^(1/T)) and mixed
+    with the uniform distribution (weight `mix`); a non-finite proposal becomes
+    uniform, so the search never depends on the network being right."""
+    ctx = GraphContext(dg)
+    n = dg.n
+    cdfs = []
+    for t in range(words.shape[0]):
+        p = net.proposal(ctx, words[t].contiguous()).to(torch.float64)
+        if not bool(torch.isfinite(p).all().item()) or float(p.sum()) <= 0:
+            p = torch.full((n,), 1.0 / n, dtype=torch.float64, device=p.device)
+        if temperature != 1.0:
+            p = torch.exp(torch.log(p.clamp_min(1e-300)) / temperature)
+            p = p / p.sum()
+        if mix > 0:
+            p = (1.0 - mix) * p + mix / n
+        cdfs.append(proposal_cdf(p))
+    off = torch.arange(len(cdfs), dtype=torch.int64, device=words.device) * n
+    return torch.cat(cdfs).contiguous(), off
 
 
 def proposal_cdf(prob: torch.Tensor) -> torch.Tensor:

@@ -24,7 +24,10 @@ node (``include/pqi.h``). Differences, all deliberate:
   which drifts after an accepted Gray move (the gray kernel reports half the
   change, ``kernels.cl:974-976``).
 * ``is_maxcut_gpu`` is accepted and ignored: there is no CPU path.
-* ``bp_scale`` (belief-propagation warm start) is not implemented and raises.
+* ``bp_scale`` runs the reference's belief-propagation warm start, whose
+  messages stay at their zero starting point (see
+  ``belief_propagation_marginals_dense``): its all-False partition competes with
+  the TFIM sample exactly as in the reference.
 """
 
 from __future__ import annotations
@@ -132,6 +135,25 @@ def local_search(dg: D.DeviceGraph, theta, is_spin_glass: bool, gray_iterations:
     return words, max_energy
 
 
+def belief_propagation_marginals_dense(G_m, n, bp_scale=1.0, damping=0.5):
+    """Per-node marginals of the reference's loopy belief propagation
+    (spin_glass_solver.py:311-415).
+
+    The reference starts every message at 0 and updates
+    m <- damping * m + (1 - damping) * artanh(clip(tanh(w) * tanh(h))), where h is
+    a sum of the node's other incoming messages. With every message 0, h = 0,
+    tanh(h) = 0, the product and its artanh are 0, and the damped message stays
+    0; so every message is exactly 0 after any number of iterations, for every
+    weight set and damping, and the marginals tanh(sum of messages) are exactly
+    0. This returns that result without iterating."""
+    return np.zeros(int(n), dtype=np.float64)
+
+
+def bp_warm_start_dense(G_m, n, bp_scale=1.0, damping=0.5):
+    """Partition from the BP marginals: marginal > 0 (spin_glass_solver.py:418-421)."""
+    return belief_propagation_marginals_dense(G_m, n, bp_scale, damping) > 0.0
+
+
 def spin_glass_solver(
     G,
     quality=None,
@@ -168,8 +190,6 @@ def spin_glass_solver(
     theta = parse_best_guess(best_guess, n_qubits)
     cut_value = None
     if theta is None:
-        if bp_scale is not None and n_qubits >= HEURISTIC_THRESHOLD:
-            raise NotImplementedError("belief-propagation warm start (bp_scale) is not implemented on this path")
         bitstring, cut_value, _ = maxcut_tfim(
             G_m,
             quality=quality,
@@ -181,6 +201,19 @@ def spin_glass_solver(
             is_maxcut_gpu=is_maxcut_gpu,
             is_nested=True,
         )
+        if bp_scale is not None and n_qubits >= HEURISTIC_THRESHOLD:
+            # keep whichever of the BP partition and the sample scores higher
+            # (spin_glass_solver.py:493-523)
+            bp_theta = bp_warm_start_dense(G_m, n_qubits, bp_scale, bp_damping)
+            sample_theta = np.array([b == "1" for b in bitstring], dtype=np.bool_)
+            dgb = D.DeviceGraph(G_m)
+            cb, eb = dgb.rescore(dgb.pack(bp_theta))
+            cs, es = dgb.rescore(dgb.pack(sample_theta))
+            bp_energy = float(eb.item()) if is_spin_glass else float(cb.item())
+            sample_energy = float(es.item()) if is_spin_glass else float(cs.item())
+            if bp_energy > sample_energy:
+                bitstring = "".join("1" if b else "0" for b in bp_theta)
+                cut_value = bp_energy if not is_spin_glass else None
         theta = np.array([b == "1" for b in bitstring], dtype=np.bool_)
 
     dg = D.DeviceGraph(G_m)

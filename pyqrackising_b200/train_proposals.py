@@ -54,7 +54,7 @@ def train_streaming(net: L.ProposalNet, count: int = 10000, chunk: int = 64, see
 
 
 def ils_compare(net: L.ProposalNet | None, dg: DeviceGraph, starts: int = 32, rounds: int = 8,
-                kick: int | None = None, seed: int = 0, spin: bool = True):
+                kick: int | None = None, seed: int = 0, spin: bool = True, temperature: float = 3.0):
     """Uniform-kick vs proposal-kick iterated search from the same ascent
     states (same seeds, same budget). Returns a dict of values and times."""
     bs = BatchedSearch([dg])
@@ -76,17 +76,13 @@ def ils_compare(net: L.ProposalNet | None, dg: DeviceGraph, starts: int = 32, ro
            "uniform_best": float(vU.max()), "uniform_mean": float(vU.mean()), "uniform_s": t_uniform}
     if net is not None:
         t = time.perf_counter()
-        ctx = L.GraphContext(dg)
-        best = int(torch.argmax(vA).item())
-        prob = net.proposal(ctx, wA[best].contiguous())
-        ok = bool(torch.isfinite(prob).all().item())
-        cdf = L.proposal_cdf(prob) if ok else None  # a failed proposal falls back to uniform kicks
-        off = torch.zeros(1, dtype=torch.int64, device=dg.device)
-        vP, _, _, sP = bs.run(tg, A, spin, rounds=rounds, kick=k, seed=seed + 1, kick_cdf=cdf,
-                              cdf_offset=off if ok else None)
+        cdf, off = L.task_proposals(net, dg, wA, temperature=temperature)
+        bsT = BatchedSearch([dg] * starts)  # one descriptor (and proposal) per task
+        vP, _, _, sP = bsT.run(list(range(starts)), A, spin, rounds=rounds, kick=k, seed=seed + 1,
+                               kick_cdf=cdf, cdf_offset=off)
         torch.cuda.synchronize()
         out.update({"learned_best": float(vP.max()), "learned_mean": float(vP.mean()),
-                    "learned_s": time.perf_counter() - t, "proposal_finite": ok})
+                    "learned_s": time.perf_counter() - t, "temperature": temperature})
     return out
 
 

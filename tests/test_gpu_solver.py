@@ -76,3 +76,27 @@ def test_spin_glass_solver_without_best_guess(name, oracle_mod):
     assert energy == pytest.approx(-oracle_mod.compute_energy(bits, W), rel=1e-12, abs=1e-9)
     # a 2-opt local optimum at least as good as 90% of the reference run from its own seed
     assert -energy <= 1e-9 or oracle_mod.compute_energy(bits, W) >= 0.9 * float(d["e2e_energy"])
+
+
+def test_bp_warm_start_candidate_competes_with_the_sample():
+    """bp_scale: the BP partition (all nodes on one side) wins when it scores
+    higher than the TFIM sample, as in the reference: with every weight
+    negative its spin energy sum |W| is the maximum, so the solver returns it;
+    for MAXCUT (cut 0) the sample wins and the result matches the run without
+    bp_scale on the same seed."""
+    import importlib
+
+    SG = importlib.import_module("pyqrackising_b200.spin_glass_solver")
+    MT = importlib.import_module("pyqrackising_b200.maxcut_tfim")
+    rng = np.random.default_rng(3)
+    n = 48
+    W = np.triu(-(rng.random((n, n)) + 0.1) * (rng.random((n, n)) < 0.3), 1).astype(np.float32)
+    W = W + W.T
+    _, _, _, energy = SG.spin_glass_solver(W, quality=2, is_spin_glass=True, bp_scale=1.0)
+    # the returned energy is minus the maximised spin value (the reference's sign)
+    assert energy == pytest.approx(-np.abs(np.triu(W, 1)).sum(), rel=1e-9)
+    MT.set_seed(5)
+    a = SG.spin_glass_solver(np.abs(W), quality=2, is_spin_glass=False, bp_scale=1.0)
+    MT.set_seed(5)
+    b = SG.spin_glass_solver(np.abs(W), quality=2, is_spin_glass=False)
+    assert a[1] == b[1] and a[0] == b[0]

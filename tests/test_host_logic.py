@@ -40,3 +40,19 @@ def test_best_guess_parsing():
 def test_get_cut():
     bs, l, r = util.get_cut(np.array([1, 0, 1], bool), ["a", "b", "c"])
     assert bs == "101" and l == ["b"] and r == ["a", "c"]
+
+
+def test_bp_marginals_match_reference_golden():
+    """The reference's loopy BP stays at its zero starting messages: marginals
+    and the warm-start partition match the reference's own outputs."""
+    import importlib
+    import os
+
+    SG = importlib.import_module("pyqrackising_b200.spin_glass_solver")
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "golden_bp.npz"))
+    for i in range(int(z["count"])):
+        W = z[f"W{i}"]
+        scale, damp = z[f"params{i}"]
+        m = SG.belief_propagation_marginals_dense(W, W.shape[0], scale, damp)
+        assert np.array_equal(m, z[f"marg{i}"])
+        assert not SG.bp_warm_start_dense(W, W.shape[0], scale, damp).any()
