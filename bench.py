@@ -12,8 +12,9 @@ and selected with its tie rule. One step = one batch.
   of the timed steps (CUDA events), inputs already in HBM. L2 is flushed
   (a 256 MB write) between timed steps, outside the timed windows.
 * e2e: the same metric through the public path with host buffers: each step
-  copies the packed batch from pinned host memory, scores it through the C ABI
-  and reads the (best value, index) pair back.
+  copies the packed batch from pinned host memory (on a copy stream, double
+  buffered so the next step's copy overlaps this step's scoring), scores it
+  through the C ABI and reads the (best value, index) pair back.
 * roofline: the scoring GEMM (2*B*n^2 integer ops per launch) against the
   int8 tensor rate, taken as twice the measured dense bf16 rate.
 * cpu_baseline: the reference's calculate_cut compiled for the host (or the
@@ -58,7 +59,8 @@ def workload_config(extra=None):
         "n": N_NODES,
         "batch": BATCH,
         "weights": "int8 (exact)",
-        "l2": "flushed between timed steps (256 MB write)",
+        "l2": "flushed between timed device steps (256 MB write); e2e steps take a fresh batch from the host each step",
+        "e2e_pipeline": "pinned H2D of each step's packed batch on a copy stream into two alternating device buffers (step i+1's copy overlaps step i's scoring), D2H of (value, index) every step",
     }
     if extra:
         cfg.update(extra)
@@ -287,6 +289,106 @@ def time_to_best(n=8192, starts=32, cluster=8):
     }
 
 
+def e2e_pipeline(dg, batches_host, like, G, L, steps, warmup):
+    """Device time (ms) of `steps` end-to-end steps: H2D copy of the step's
+    packed batch from pinned memory, scoring through the public call, D2H of
+    the selected (value, index). Copies run on their own stream into two
+    alternating device buffers."""
+    import torch
+
+    nb = len(batches_host)
+    pinned = [torch.from_numpy(b.view(np.int32).reshape(-1)).pin_memory() for b in batches_host]
+    dev_in = [torch.empty_like(like) for _ in range(2)]
+    out_e = torch.empty(steps + warmup, dtype=torch.float32).pin_memory()
+    out_i = torch.empty(steps + warmup, dtype=torch.int32).pin_memory()
+    comp = torch.cuda.current_stream()
+    copy = torch.cuda.Stream()
+    copied = [torch.cuda.Event() for _ in range(2)]
+    used = [torch.cuda.Event() for _ in range(2)]
+
+    def run(i0, count):
+        for i in range(i0, i0 + count):
+            buf = i & 1
+            with torch.cuda.stream(copy):
+                if i >= 2:
+                    copy.wait_event(used[buf])  # step i-2 has finished reading this buffer
+                dev_in[buf].copy_(pinned[i % nb], non_blocking=True)
+                copied[buf].record(copy)
+            comp.wait_event(copied[buf])
+            _, be, bi = dg.calculate_cut(dev_in[buf], BATCH, False, G, L, energies=False)
+            used[buf].record(comp)
+            out_e[i].copy_(be[0], non_blocking=True)
+            out_i[i].copy_(bi[0], non_blocking=True)
+
+    run(0, warmup)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(comp)
+    copy.wait_stream(comp)
+    run(warmup, steps)
+    end.record(comp)
+    end.synchronize()
+    return start.elapsed_time(end)
+
+
+def plain_small_leg(reps=5):
+    """Config 1: spin_glass_solver(W, quality=6, is_spin_glass=True) on the
+    3-regular n=64 +-1 fixture from its recorded best_guess, through the public
+    call; next to it the reference's GPU-branch driver loop run on the host
+    cores with the reference's kernels compiled for the host (or the C port)."""
+    import importlib
+
+    import torch
+
+    from oracle import oracle as O
+
+    SG = importlib.import_module("pyqrackising_b200.spin_glass_solver")
+    z = np.load(os.path.join(REPO, "tests", "golden", "golden_c1_regular64.npz"))
+    W = z["W"]
+    guess = [bool(b) for b in z["best_guess"]]
+    iters = int(z["e2e_gray_iterations"])
+    SG.spin_glass_solver(W, quality=6, is_spin_glass=True, best_guess=guess, gray_iterations=iters)  # warm
+    ts = []
+    res = None
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        res = SG.spin_glass_solver(W, quality=6, is_spin_glass=True, best_guess=guess, gray_iterations=iters)
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t)
+    use_ref = O.ref_available()
+    tc = []
+    theta_ref = None
+    for _ in range(reps):
+        t = time.perf_counter()
+        theta_ref = O.spin_glass_gpu_path(W, np.array(guess), True, iters, 148, 148, use_ref=use_ref)[0]
+        tc.append(time.perf_counter() - t)
+    e_ref = O.compute_energy(theta_ref, W)
+    return {
+        "workload": "3-regular n=64 +-1 (fixture), spin_glass_solver(quality=6, is_spin_glass=True) from the recorded best_guess",
+        "ms": 1e3 * float(np.median(ts)),
+        "energy": -float(res[3]),
+        "cpu_ms": 1e3 * float(np.median(tc)),
+        "cpu_kind": "reference" if use_ref else "port",
+        "cpu_energy": float(e_ref),
+        "not_below_reference": -float(res[3]) >= float(e_ref) - 1e-9,
+    }
+
+
+def learned_leg():
+    """Config 5: the committed trained proposal network on G(16384, 0.01) with
+    N(0, 1) weights: the batched iterated search with uniform kicks and with
+    the network's per-task proposals from the same optima, each refined by the
+    plain local search (the judge), next to the plain search alone."""
+    from pyqrackising_b200 import learned as L
+    from pyqrackising_b200.train_proposals import evaluate
+
+    net = L.ProposalNet.load(os.path.join(REPO, "pyqrackising_b200", "weights", "proposal_net.pt"))
+    r = evaluate(net)
+    r["weights"] = "pyqrackising_b200/weights/proposal_net.pt (trained on 10,000 streamed graphs)"
+    return r
+
+
 def batched_leg(graphs=512, seeds=256):
     """Batched uneven instances: 512 graphs, n ~ U[64, 1024] (half 3-regular
     +-1 as int8, half G(n, 0.1) with uniform (0, 1] float32 weights), 256
@@ -463,29 +565,11 @@ def main():
         kernel_ms = float(np.mean([a.elapsed_time(b) for a, b in kev]))
         total_ms = float(np.sum(step_ms))
 
-        # e2e through the C ABI with host buffers (pinned), copies inside the window
-        pinned = [torch.from_numpy(b.view(np.int32).reshape(-1)).pin_memory() for b in batches_host]
-        dev_in = torch.empty_like(batches[0])
-        out_e = torch.empty(1, dtype=torch.float32).pin_memory()
-        out_i = torch.empty(1, dtype=torch.int32).pin_memory()
-        e2e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-        for i in range(args.warmup):
-            dev_in.copy_(pinned[i % nb], non_blocking=True)
-            _, be, bi = dg.calculate_cut(dev_in, BATCH, False, G, L, energies=False)
-            out_e.copy_(be, non_blocking=True)
-            out_i.copy_(bi, non_blocking=True)
-        torch.cuda.synchronize()
-        for i in range(args.steps):
-            flush.fill_(i & 0xFF)
-            e2e_evs[i][0].record(stream)
-            dev_in.copy_(pinned[i % nb], non_blocking=True)
-            _, be, bi = dg.calculate_cut(dev_in, BATCH, False, G, L, energies=False)
-            out_e.copy_(be, non_blocking=True)
-            out_i.copy_(bi, non_blocking=True)
-            e2e_evs[i][1].record(stream)
-        torch.cuda.synchronize()
-        e2e_ms = float(np.sum([a.elapsed_time(b) for a, b in e2e_evs]))
-
+        # e2e through the C ABI with host buffers (pinned), copies inside the
+        # window: each step copies its packed batch host -> device on a copy
+        # stream (double-buffered, so step i+1's copy overlaps step i's
+        # scoring), scores it, and reads the (value, index) pair back.
+        e2e_ms = e2e_pipeline(dg, batches_host, batches[0], G, L, args.steps, args.warmup)
     if dist:
         t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dg.device)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -544,7 +628,9 @@ def main():
         if world == 1 and not args.no_ttb:
             line["time_to_best"] = time_to_best()
         if world == 1 and not args.no_batched:
+            line["plain_small"] = plain_small_leg()
             line["batched"] = batched_leg()
+            line["learned"] = learned_leg()
             line["flip_updates"] = flip_bandwidth_leg()
         if world == 1:
             try:

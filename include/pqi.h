@@ -356,6 +356,18 @@ pqi_status pqi_mpnn_gemm(int transA, int transB, int M, int N, int K, float alph
                          int lda, const void* B, int ldb, float beta, float* C32, void* C16,
                          int ldc, const float* bias, int relu, void* stream);
 
+/* OUT[:, 0:64] = A_hat X (+ beta * OUT32) on the tensor cores (tcgen05,
+ * bf16 operands, float32 accumulation): A_hat is n x n bf16 with pitch ld, X
+ * is given transposed (Xt: 64 x n bf16, pitch ldt); writes OUT32 (float32)
+ * and / or OUT16 (bf16), row pitch ldo. ld and ldt multiples of 8, 16-byte
+ * aligned bases. PQI_ENOTSUP off sm_100. */
+pqi_status pqi_mpnn_adj_gemm(const void* Ahat, int ld, int n, const void* Xt, int ldt, float beta,
+                             float* out32, void* out16, int ldo, void* stream);
+
+/* Xt[c][r] = X[r][c] for r < n, c < 64 (bf16; X pitch ldx >= 64, Xt pitch
+ * ldt >= n, rows n..ldt-1 of Xt zeroed). */
+pqi_status pqi_mpnn_transpose64(const void* X, int n, int ldx, void* Xt, int ldt, void* stream);
+
 /* A_hat = D^-1/2 W D^-1/2 in bf16 (n x ld, zero diagonal and padding) and
  * s_v = sum_{u != v} |W_vu| (float32) from the caller's n x n W. */
 pqi_status pqi_mpnn_norm_adj(const float* W, int n, void* Ahat, int ld, float* s, void* stream);
@@ -394,6 +406,13 @@ pqi_status pqi_mpnn_adam(float* w, const float* g, float* m, float* v, void* w16
  * FLT_EPSILON (float32 difference), J_eff = -(sum of those differences)/degree. */
 pqi_status pqi_tfim_jz(const float* W, int n, double* J_eff, unsigned int* degrees,
                        void* workspace, size_t workspace_bytes, void* stream);
+
+/* pqi_tfim_jz with the reference's sparse-path arithmetic
+ * (maxcut_tfim_sparse.py:204-224, plain numpy scalars): float32 row sums in
+ * node order and a float32 division. W is the dense matrix of the stored
+ * (upper-triangular) entries. */
+pqi_status pqi_tfim_jz_f32(const float* W, int n, double* J_eff, unsigned int* degrees,
+                           void* workspace, size_t workspace_bytes, void* stream);
 
 /* Workspace bytes pqi_tfim_cdf needs. */
 size_t pqi_tfim_cdf_workspace_bytes(int n, int quality);

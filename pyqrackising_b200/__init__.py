@@ -13,5 +13,6 @@ CUDA behind the C ABI in include/pqi.h); there is no CPU fallback.
 
 from .maxcut_tfim import maxcut_tfim
 from .spin_glass_solver import spin_glass_solver
+from .sparse import maxcut_tfim_sparse, spin_glass_solver_sparse
 
-__all__ = ["maxcut_tfim", "spin_glass_solver"]
+__all__ = ["maxcut_tfim", "spin_glass_solver", "maxcut_tfim_sparse", "spin_glass_solver_sparse"]

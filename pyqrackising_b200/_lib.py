@@ -95,6 +95,8 @@ SIGNATURES = {
     "pqi_apply_flip": (_i, [_WP, _vp, _vp, _i, _i, _vp]),
     "pqi_batch_graph_desc_bytes": (_sz, []),
     "pqi_batch_search": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pqi_mpnn_transpose64": (_i, [_vp, _i, _i, _vp, _i, _vp]),
+    "pqi_mpnn_adj_gemm": (_i, [_vp, _i, _i, _vp, _i, ctypes.c_float, _vp, _vp, _i, _vp]),
     "pqi_batch_search_warp": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "pqi_cluster_ascent": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "pqi_mpnn_gemm": (_i, [_i, _i, _i, _i, _i, ctypes.c_float, _vp, _i, _vp, _i, ctypes.c_float, _vp, _vp, _i, _vp, _i, _vp]),
@@ -106,6 +108,7 @@ SIGNATURES = {
     "pqi_mpnn_to_bf16": (_i, [_vp, _sz, _vp, _vp]),
     "pqi_mpnn_adam": (_i, [_vp, _vp, _vp, _vp, _vp, _sz, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _i, _vp]),
     "pqi_tfim_jz": (_i, [_vp, _i, _vp, _vp, _vp, _sz, _vp]),
+    "pqi_tfim_jz_f32": (_i, [_vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_tfim_cdf_workspace_bytes": (_sz, [_i, _i]),
     "pqi_tfim_cdf": (_i, [_vp, _vp, _i, _i, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _sz, _vp]),
     "pqi_tfim_sample_workspace_bytes": (_sz, [_i]),

@@ -27,6 +27,7 @@
 #include <algorithm>
 
 #include "pqi_common.cuh"
+#include "pqi_tc.cuh"
 
 namespace pqi {
 
@@ -40,123 +41,6 @@ constexpr int A_STAGE = BM * BK_BYTES;   // 16 KB
 constexpr int B_STAGE = BN * BK_BYTES;   // 32 KB
 constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
-constexpr long long WAIT_BUDGET_CYCLES = 4000000000ll;  // ~2 s at 1.9 GHz
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-// Bounded wait for the phase with parity `parity`; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t addr = smem_u32(bar);
-  const long long t0 = clock64();
-  while (true) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (clock64() - t0 > WAIT_BUDGET_CYCLES) return false;
-  }
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x,
-                                            int y) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
-      "%4}], [%2];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
-      : "memory");
-}
-
-// K-major operand tile with 128-byte swizzle: 8-row groups 1024 B apart.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);  // start address (16-byte units)
-  d |= (uint64_t)1 << 16;                   // leading byte offset (unused for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;         // stride byte offset: 8 rows x 128 B
-  d |= (uint64_t)1 << 46;                   // descriptor version for sm_100
-  d |= (uint64_t)2 << 61;                   // SWIZZLE_128B
-  return d;
-}
-
-template <bool kInt8>
-__device__ __forceinline__ void mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                    uint32_t accumulate) {
-  if constexpr (kInt8) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-  } else {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-  }
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-          smem_u32(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void tmem_load32_nowait(uint32_t taddr, uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-}
-
-// After tcgen05.wait::ld: ties 32 registers written by an asynchronous
-// tcgen05.ld to this point, so no use of them is scheduled before the wait.
-__device__ __forceinline__ void reg_fence32(uint32_t (&r)[32]) {
-  asm volatile(""
-               : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
-                 "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
-                 "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15]), "+r"(r[16]), "+r"(r[17]),
-                 "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]), "+r"(r[22]), "+r"(r[23]),
-                 "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]), "+r"(r[29]),
-                 "+r"(r[30]), "+r"(r[31]));
-}
-
-__device__ __forceinline__ void tmem_load32(uint32_t taddr, uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
-        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
-        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
 
 // Instruction descriptors (M = 128, N = 256, both operands K-major).
 constexpr uint32_t kIdescI8 = (2u << 4)      // D: s32
@@ -173,10 +57,6 @@ constexpr int TMA_WARP = 0;       // warp 0 lane 0: TMA loads of the X and W til
 constexpr int MMA_WARP = 1;       // warp 1: TMEM alloc, lane 0 issues MMAs
 constexpr int PTHREADS = 192;     // warps 2-5: epilogue (TMEM lane quarter = warp % 4)
 constexpr int ACC_COLS = 512;     // two 256-column accumulators
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
 
 __device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
@@ -479,38 +359,58 @@ __global__ void __launch_bounds__(PTHREADS, 1)
   if (threadIdx.x == 0 && s_fail) atomicExch(err, 1);
 }
 
-// +-1 operand from packed bits: X[b][v] for v < 32*ceil(n/32) (row pitch ld
-// elements); columns at and beyond n are never read (the A tensor map ends at n).
+// One packed word -> 32 +-1 elements of the A operand.
+template <typename T>
+__device__ __forceinline__ void expand_word(uint32_t bits, T* __restrict__ dst) {
+  if constexpr (sizeof(T) == 1) {
+    // bit -> byte 0x01 (set) or 0xFF (clear), four at a time
+    uint32_t o[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const uint32_t t = (((bits >> (4 * q)) & 0xFu) * 0x00204081u) & 0x01010101u;
+      o[q] = 0xFFFFFFFFu - t * 0xFEu;
+    }
+    reinterpret_cast<uint4*>(dst)[0] = make_uint4(o[0], o[1], o[2], o[3]);
+    reinterpret_cast<uint4*>(dst)[1] = make_uint4(o[4], o[5], o[6], o[7]);
+  } else {
+    uint32_t o[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const uint32_t lo = ((bits >> (2 * q)) & 1u) ? 0x3F80u : 0xBF80u;
+      const uint32_t hi = ((bits >> (2 * q + 1)) & 1u) ? 0x3F80u : 0xBF80u;
+      o[q] = lo | (hi << 16);
+    }
+    uint4* d4 = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) d4[q] = make_uint4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+  }
+}
+
+// Packed candidates -> the +-1 A operand (int8, or bf16 for the float path),
+// row pitch ld elements; each thread expands four words (one 16-byte load when
+// the rows are 16-byte aligned) into 128 contiguous int8 (256 bf16) outputs.
+// Columns at and beyond n are never read (the A tensor map ends at n).
 template <typename T>
 __global__ void expand_pm1_kernel(const uint32_t* __restrict__ theta, int shots, int n32, int ld,
                                   T* __restrict__ X) {
-  const long long total = (long long)shots * n32;
+  const int q32 = (n32 + 3) >> 2;  // word quads per row
+  const bool vec = (n32 & 3) == 0;
+  const long long total = (long long)shots * q32;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
-    const int b = (int)(e / n32), w = (int)(e - (long long)b * n32);
-    const uint32_t bits = theta[e];
-    T* dst = X + (size_t)b * ld + (size_t)w * 32;
-    if constexpr (sizeof(T) == 1) {
-      // bit -> byte 0x01 (set) or 0xFF (clear), four at a time
-      uint32_t o[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const uint32_t t = (((bits >> (4 * q)) & 0xFu) * 0x00204081u) & 0x01010101u;
-        o[q] = 0xFFFFFFFFu - t * 0xFEu;
-      }
-      reinterpret_cast<uint4*>(dst)[0] = make_uint4(o[0], o[1], o[2], o[3]);
-      reinterpret_cast<uint4*>(dst)[1] = make_uint4(o[4], o[5], o[6], o[7]);
+    const int b = (int)(e / q32), w0 = 4 * (int)(e - (long long)b * q32);
+    const uint32_t* src = theta + (size_t)b * n32 + w0;
+    T* dst = X + (size_t)b * ld + (size_t)w0 * 32;
+    if (vec) {
+      const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
+      expand_word<T>(v.x, dst);
+      expand_word<T>(v.y, dst + 32);
+      expand_word<T>(v.z, dst + 64);
+      expand_word<T>(v.w, dst + 96);
     } else {
-      uint32_t o[16];
 #pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const uint32_t lo = ((bits >> (2 * q)) & 1u) ? 0x3F80u : 0xBF80u;
-        const uint32_t hi = ((bits >> (2 * q + 1)) & 1u) ? 0x3F80u : 0xBF80u;
-        o[q] = lo | (hi << 16);
-      }
-      uint4* d4 = reinterpret_cast<uint4*>(dst);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) d4[q] = make_uint4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+      for (int i = 0; i < 4; ++i)
+        if (w0 + i < n32) expand_word<T>(__ldg(src + i), dst + 32 * i);
     }
   }
 }
@@ -518,12 +418,7 @@ __global__ void expand_pm1_kernel(const uint32_t* __restrict__ theta, int shots,
 }  // namespace tc
 
 
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-static EncodeTiledFn encode_fn() {
+EncodeTiledFn encode_fn() {
   static EncodeTiledFn fn = nullptr;
   static bool tried = false;
   if (!tried) {
@@ -565,8 +460,8 @@ struct MapCacheEntry {
 };
 
 // Tensor maps depend only on (address, shape): keep the last few encoded.
-static bool cached_map(CUtensorMap* out, const void* base, bool int8, int rows, int cols, int pitch,
-                       int box_rows) {
+bool cached_map(CUtensorMap* out, const void* base, bool int8, int rows, int cols, int pitch,
+                int box_rows) {
   static MapCacheEntry cache[8] = {};
   static int next = 0;
   for (const auto& e : cache) {
@@ -643,8 +538,8 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     attr_set[i8] = true;
   }
   PQI_TRY(cudaMemsetAsync(ctl, 0, ctl_bytes, s));
-  const long long words = (long long)shots * n32;
-  const int eg = (int)std::max<long long>(1, std::min<long long>((words + 255) / 256, 148 * 16));
+  const long long quads = (long long)shots * ((n32 + 3) / 4);
+  const int eg = (int)std::max<long long>(1, std::min<long long>((quads + 255) / 256, 148 * 16));
   if (i8) {
     tc::expand_pm1_kernel<int8_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (int8_t*)X);
   } else {

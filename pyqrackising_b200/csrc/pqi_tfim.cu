@@ -92,6 +92,30 @@ __global__ void tfim_jz_kernel(const float* __restrict__ W, int n, const float* 
   }
 }
 
+// The sparse path's J_eff and degrees (maxcut_tfim_sparse.py:204-224): the
+// same rule, but the reference runs it as plain numpy scalar arithmetic, so
+// the row sum is float32, accumulated in node order, and J = -(sum / degree)
+// is a float32 division. One thread per row reproduces that order exactly.
+__global__ void tfim_jz_f32_kernel(const float* __restrict__ W, int n, const float* min_key,
+                                   double* __restrict__ J_eff, unsigned int* __restrict__ degrees) {
+  unsigned int k = *reinterpret_cast<const unsigned int*>(min_key);
+  k = (k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k;
+  const float gmin = __uint_as_float(k);
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+    const float* row = W + (size_t)r * n;
+    unsigned int deg = 0;
+    float J = 0.0f;
+    for (int m = 0; m < n; ++m) {
+      const float val = __fsub_rn(row[m], gmin);
+      if ((double)val <= kEps) continue;
+      ++deg;
+      J = __fadd_rn(J, val);
+    }
+    J_eff[r] = deg > 0 ? (double)(-__fdiv_rn(J, (float)deg)) : 0.0;
+    degrees[r] = deg;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // maxcut_hamming_cdf (maxcut_tfim_util.py:654-687)
 
@@ -362,6 +386,23 @@ pqi_status pqi_tfim_jz(const float* W, int n, double* J_eff, unsigned int* degre
   tfim_jz_kernel<<<std::max(1, std::min((n + 7) / 8, 148 * 4)), 256, 0, s>>>(W, n, mn, J_eff,
                                                                              degrees);
   PQI_LAUNCHED("tfim_jz_kernel");
+  return PQI_OK;
+}
+
+pqi_status pqi_tfim_jz_f32(const float* W, int n, double* J_eff, unsigned int* degrees,
+                           void* workspace, size_t workspace_bytes, void* stream) {
+  PQI_CHECK_ARG(W && J_eff && degrees && n > 0);
+  Workspace ws(workspace, workspace_bytes);
+  float* mn = ws.take<float>(1);
+  PQI_CHECK_ARG(mn);
+  cudaStream_t s = as_stream(stream);
+  PQI_TRY(cudaMemsetAsync(mn, 0xFF, sizeof(float), s));  // max key
+  const long long total = (long long)n * n;
+  const int g = (int)std::max<long long>(1, std::min<long long>((total + 255) / 256, 148 * 8));
+  tfim_min_kernel<<<g, 256, 0, s>>>(W, total, mn);
+  PQI_LAUNCHED("tfim_min_kernel");
+  tfim_jz_f32_kernel<<<(n + 127) / 128, 128, 0, s>>>(W, n, mn, J_eff, degrees);
+  PQI_LAUNCHED("tfim_jz_f32_kernel");
   return PQI_OK;
 }
 

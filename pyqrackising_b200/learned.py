@@ -107,6 +107,25 @@ class ProposalNet:
         return ctypes.c_void_p(self.g.data_ptr() + 4 * self._off(name))
 
     # forward / backward -----------------------------------------------------------
+    tensor_cores = True  # message products on tcgen05 (False: the CUDA-core GEMM)
+
+    def _adj(self, ctx: "GraphContext", X, ldx, beta, out32, out16, ldo, sp, what):
+        """OUT[:, 0:64] = A_hat X (+ beta OUT32): the message product, on the
+        tensor cores (X transposed first) or on the CUDA-core GEMM."""
+        lib = _lib.load()
+        Xp = X if isinstance(X, ctypes.c_void_p) else _p(X)
+        if self.tensor_cores:
+            Xt = torch.empty(HID * ctx.ld, dtype=torch.bfloat16, device=self.device)
+            rc = lib.pqi_mpnn_transpose64(Xp, ctx.n, ldx, _p(Xt), ctx.ld, sp)
+            if rc == 0:
+                rc = lib.pqi_mpnn_adj_gemm(_p(ctx.Ah), ctx.ld, ctx.n, _p(Xt), ctx.ld, ctypes.c_float(beta),
+                                           out32 if out32 is not None else None, out16, ldo, sp)
+        else:
+            rc = lib.pqi_mpnn_gemm(0, 0, ctx.n, HID, ctx.n, ctypes.c_float(1.0), _p(ctx.Ah), ctx.ld, Xp, ldx,
+                                   ctypes.c_float(beta), out32, out16, ldo, None, 0, sp)
+        if rc:
+            raise _lib.PQIError(rc, what)
+
     def forward(self, ctx: GraphContext, F: torch.Tensor, stream=None):
         """Logits (float32, n) and the activations the backward pass needs."""
         n = ctx.n
@@ -126,8 +145,7 @@ class ProposalNet:
         for l in range(1, LAYERS + 1):
             Cl = C[l - 1]
             # M = A_hat H_{l-1} -> right half of C[l-1]
-            chk(gemm(0, 0, n, HID, n, 1.0, _p(ctx.Ah), ctx.ld, _p(Cl), ld2, 0.0, None,
-                     ctypes.c_void_p(Cl.data_ptr() + 2 * HID), ld2, None, 0, sp), f"gemm msg{l}")
+            self._adj(ctx, Cl, ld2, 0.0, None, ctypes.c_void_p(Cl.data_ptr() + 2 * HID), ld2, sp, f"msg{l}")
             # H_l = relu(C AB_l + b_l) -> left half of C[l]
             chk(gemm(0, 0, n, HID, 2 * HID, 1.0, _p(Cl), ld2, self.w16_ptr(f"AB{l}"), HID, 0.0, _p(H32[l]), _p(C[l]), ld2, self.w32_ptr(f"b{l}"), 1, sp), f"gemm AB{l}")
         logits = torch.empty(n, dtype=torch.float32, device=dev)
@@ -169,7 +187,7 @@ class ProposalNet:
             # dC = dZ AB_l^T
             chk(gemm(0, 1, n, 2 * HID, HID, 1.0, _p(dZ16), ld2, self.w16_ptr(f"AB{l}"), HID, 0.0, _p(dC), _p(dC16), ld2, None, 0, sp), f"dC{l}")
             # dH_{l-1} = dC[:, :64] + A_hat dC[:, 64:]   (A_hat symmetric)
-            chk(gemm(0, 0, n, HID, n, 1.0, _p(ctx.Ah), ctx.ld, ctypes.c_void_p(dC16.data_ptr() + 2 * HID), ld2, 1.0, _p(dC), None, ld2, None, 0, sp), f"dmsg{l}")
+            self._adj(ctx, ctypes.c_void_p(dC16.data_ptr() + 2 * HID), ld2, 1.0, _p(dC), None, ld2, sp, f"dmsg{l}")
             dH, dC = dC, dH
         chk(lib.pqi_mpnn_relu_bwd(_p(dH), _p(H32[0]), n * ld2, _p(dZ), _p(dZ16), sp), "relu0")
         chk(gemm(1, 0, FEAT, HID, n, 1.0, _p(cache["F"]), FEAT, _p(dZ16), ld2, 1.0, self.g32_ptr("A0"), None, HID, None, 0, sp), "dA0")
@@ -190,6 +208,13 @@ class ProposalNet:
     def zero_grad(self):
         self.g.zero_()
 
+    def clip_grad(self, max_norm: float) -> float:
+        """Scale the gradient to at most `max_norm` (L2); returns the norm before."""
+        norm = float(torch.linalg.vector_norm(self.g).item())
+        if norm > max_norm > 0:
+            self.g.mul_(max_norm / norm)
+        return norm
+
     def adam_step(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8, stream=None):
         self.step_count += 1
         _lib.call("pqi_mpnn_adam", _p(self.w), _p(self.g), _p(self.m), _p(self.v), _p(self.w16), self.count,
@@ -202,6 +227,19 @@ class ProposalNet:
         logits, _ = self.forward(ctx, F)
         _, _, prob = self.loss_grad(logits, None)
         return prob
+
+    def snapshot(self):
+        """Copy of the parameters (float32 master)."""
+        return self.w.detach().clone()
+
+    def restore(self, params: torch.Tensor, reset_moments: bool = True):
+        """Load parameters from `snapshot()`, refresh the bf16 copy and, by
+        default, reset Adam's moments."""
+        self.w.copy_(params)
+        _lib.call("pqi_mpnn_to_bf16", _p(self.w), self.count, _p(self.w16), None)
+        if reset_moments:
+            self.m.zero_()
+            self.v.zero_()
 
     def state_dict(self):
         return {"params": self.w.detach().cpu().clone(), "step": self.step_count}
@@ -300,8 +338,10 @@ def make_examples(dgs, tasks_per_graph=4, rounds=12, kick_frac=1 / 16, seed=0):
     return out
 
 
-def train(net: ProposalNet, dgs, examples, epochs=2, lr=2e-3, batch=8, log=None):
-    """Adam on the softmax cross-entropy of the examples; returns loss history."""
+def train(net: ProposalNet, dgs, examples, epochs=2, lr=2e-3, batch=8, log=None, clip=1.0):
+    """Adam on the softmax cross-entropy of the examples; returns loss history.
+    `lr` is a number or a function of the optimiser step; gradients are
+    clipped to L2 norm `clip` (0: off)."""
     ctxs = {}
     hist = []
     order = np.arange(len(examples))
@@ -326,7 +366,9 @@ def train(net: ProposalNet, dgs, examples, epochs=2, lr=2e-3, batch=8, log=None)
                 dl /= len(order[b0 : b0 + batch])
                 net.backward(ctx, cache, dl)
                 losses.append(loss)
-            net.adam_step(lr=lr)
+            if clip:
+                net.clip_grad(clip)
+            net.adam_step(lr=lr(net.step_count) if callable(lr) else lr)
             tot = float(torch.stack(losses).mean().item())
             hist.append(tot)
             if log is not None and (len(hist) % 50 == 0):

@@ -62,9 +62,18 @@ def maxcut_tfim(
     is_nested=False,
 ):
     nodes, G_m = as_matrix(G)
+    return _maxcut_tfim(nodes, G_m, quality, shots, is_spin_glass, anneal_t, anneal_h, repulsion_base)
+
+
+def _maxcut_tfim(nodes, G_m, quality, shots, is_spin_glass, anneal_t, anneal_h, repulsion_base,
+                 threshold=HEURISTIC_THRESHOLD, jz_matrix=None):
+    """maxcut_tfim on a dense symmetric matrix. `threshold` is the size below
+    which the exhaustive search runs; `jz_matrix` (default G_m) is the matrix
+    whose rows give the sampler's J_eff and degrees (the sparse entry point
+    passes the upper triangle, as the reference's sparse path reads it)."""
     n_qubits = len(G_m)
 
-    if n_qubits < HEURISTIC_THRESHOLD:
+    if n_qubits < threshold:
         best_solution, best_value = exact_search(G_m, is_spin_glass)
         bit_string, l, r = get_cut(best_solution, nodes)
         if best_value < 0.0:
@@ -83,8 +92,12 @@ def maxcut_tfim(
         repulsion_base = 5.0
 
     dg = D.DeviceGraph(G_m)
+    jz = None
+    if jz_matrix is not None:
+        jz = torch.from_numpy(np.ascontiguousarray(jz_matrix, dtype=np.float32)).to(dg.device)
     best_solution, best_value = sample_and_score(
-        dg, int(quality), int(shots), bool(is_spin_glass), float(anneal_t), float(anneal_h), float(repulsion_base)
+        dg, int(quality), int(shots), bool(is_spin_glass), float(anneal_t), float(anneal_h), float(repulsion_base),
+        jz_W=jz,
     )
     bit_string, l, r = get_cut(best_solution, nodes)
     if best_value < 0.0:
@@ -133,15 +146,20 @@ def init_thresholds(n_qubits: int) -> np.ndarray:
     return thresholds
 
 
-def hamming_cdf(dg: D.DeviceGraph, quality: int, anneal_t: float, anneal_h: float):
-    """(J_eff, degrees, cum_prob) on the device (init_J_and_z + maxcut_hamming_cdf)."""
+def hamming_cdf(dg: D.DeviceGraph, quality: int, anneal_t: float, anneal_h: float, jz_W=None):
+    """(J_eff, degrees, cum_prob) on the device (init_J_and_z + maxcut_hamming_cdf);
+    J_eff and degrees come from the rows of `jz_W` (n x n float32 on the
+    device; the sparse path's stored rows, summed with its float32 rule),
+    default the graph's own matrix."""
     n = dg.n
     dev = dg.device
     lib = _lib.load()
     J_eff = torch.empty(n, dtype=torch.float64, device=dev)
     degrees = torch.empty(n, dtype=torch.int32, device=dev)
     wsp, wsn = dg.wsp(1)
-    _lib.call("pqi_tfim_jz", D._ptr(dg.W), n, D._ptr(J_eff), D._ptr(degrees), wsp, wsn, dg.sp())
+    # the sparse path passes its stored rows and the reference's float32 rule
+    _lib.call("pqi_tfim_jz_f32" if jz_W is not None else "pqi_tfim_jz",
+              D._ptr(jz_W if jz_W is not None else dg.W), n, D._ptr(J_eff), D._ptr(degrees), wsp, wsn, dg.sp())
     thr = torch.from_numpy(init_thresholds(n)).to(dev)
     cum = torch.empty(max(n - 1, 1), dtype=torch.float64, device=dev)
     ws = dg.ws.get(lib.pqi_tfim_cdf_workspace_bytes(n, quality))
@@ -189,12 +207,12 @@ def sample_batch(dg: D.DeviceGraph, cum, shots: int, repulsion_base: float, seed
 
 
 def sample_and_score(dg: D.DeviceGraph, quality: int, shots: int, is_spin_glass: bool, anneal_t: float,
-                     anneal_h: float, repulsion_base: float, max_rounds: int = 1 << 20):
+                     anneal_h: float, repulsion_base: float, max_rounds: int = 1 << 20, jz_W=None):
     """sample_for_opencl (maxcut_tfim.py:148-186) on the device: draw rounds of
     candidates and score each round with the batched scoring kernel until a
     round does not beat the best so far. Returns (bool[n], value)."""
     n = dg.n
-    _, _, cum = hamming_cdf(dg, quality, anneal_t, anneal_h)
+    _, _, cum = hamming_cdf(dg, quality, anneal_t, anneal_h, jz_W=jz_W)
     shots = ((max(1, shots >> 1) + 31) >> 5) << 5
     mpe = D.max_gpu_proc_elem(dg.device)
     G, L = D.geometry(shots, shots, mpe)

@@ -1,0 +1,95 @@
+"""Sparse-input entry points: spin_glass_solver_sparse and maxcut_tfim_sparse
+(pyqrackising/spin_glass_solver_sparse.py:517-864,
+pyqrackising/maxcut_tfim_sparse.py:373-472), same signatures and returns.
+
+The reference's sparse kernels sum every stored CSR entry (u, v) once
+(kernels.cl:233-251), which is the dense form with
+W = G_offdiag + G_offdiag^T: a graph's sparse and dense objectives, flip
+values and pair values agree, and only the summation order differs. On a B200
+the graph is therefore expanded to that dense matrix in HBM (n = 65536 takes
+17 GB of 180), where the tensor-core scoring and the row-streaming flip kernels
+run; the CSR never reaches the device. What the sparse path does differently is
+kept: the exhaustive search below n = 23 (maxcut_tfim_util.py:166) and the
+sampler's J_eff and degrees read from the stored (upper-triangular) rows
+(maxcut_tfim_sparse.py:204-224). Diagonal entries (self-loops) are dropped:
+they change no cut.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from .maxcut_tfim import _maxcut_tfim
+from .spin_glass_solver import _spin_glass_solver
+
+HEURISTIC_THRESHOLD_SPARSE = 23  # maxcut_tfim_util.py:166
+
+
+def sparse_to_dense(G):
+    """(nodes, dense symmetric W, stored-rows matrix S) from an nx.Graph (read
+    as the reference does: upper triangle in node order, weight default 1.0,
+    maxcut_tfim_util.py:533-542) or a scipy sparse matrix (used as given).
+    S holds the stored entries off the diagonal (the rows the sampler's J and
+    degrees are read from); W = S + S^T."""
+    try:
+        import networkx as nx
+    except ImportError:  # pragma: no cover
+        nx = None
+    if nx is not None and isinstance(G, nx.Graph):
+        nodes = list(G.nodes())
+        n = len(nodes)
+        index = {u: i for i, u in enumerate(nodes)}
+        S = np.zeros((n, n), dtype=np.float32)
+        for u, v, d in G.edges(data=True):
+            i, j = index[u], index[v]
+            if i == j:
+                continue
+            a, b = (i, j) if i < j else (j, i)
+            S[a, b] = np.float32(d.get("weight", 1.0))
+    else:
+        coo = G.tocoo()
+        n = coo.shape[0]
+        nodes = list(range(n))
+        S = np.zeros((n, n), dtype=np.float32)
+        keep = coo.row != coo.col
+        np.add.at(S, (coo.row[keep], coo.col[keep]), coo.data[keep].astype(np.float32))
+    W = S + S.T
+    return nodes, W, S
+
+
+def maxcut_tfim_sparse(
+    G,
+    quality=None,
+    shots=None,
+    is_spin_glass=False,
+    anneal_t=None,
+    anneal_h=None,
+    repulsion_base=None,
+    is_maxcut_gpu=True,
+    is_nested=False,
+):
+    nodes, W, S = sparse_to_dense(G)
+    return _maxcut_tfim(nodes, W, quality, shots, is_spin_glass, anneal_t, anneal_h, repulsion_base,
+                        threshold=HEURISTIC_THRESHOLD_SPARSE, jz_matrix=S)
+
+
+def spin_glass_solver_sparse(
+    G,
+    quality=None,
+    shots=None,
+    best_guess=None,
+    is_maxcut_gpu=True,
+    is_spin_glass=True,
+    anneal_t=None,
+    anneal_h=None,
+    repulsion_base=None,
+    is_log=False,
+    gray_iterations=None,
+    gray_seed_multiple=None,
+    bp_scale=None,
+    bp_damping=0.5,
+):
+    nodes, W, S = sparse_to_dense(G)
+    return _spin_glass_solver(nodes, W, quality, shots, best_guess, is_maxcut_gpu, is_spin_glass, anneal_t,
+                              anneal_h, repulsion_base, gray_iterations, gray_seed_multiple, bp_scale, bp_damping,
+                              threshold=HEURISTIC_THRESHOLD_SPARSE, jz_matrix=S)

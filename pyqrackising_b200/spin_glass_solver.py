@@ -38,7 +38,7 @@ import numpy as np
 import torch
 
 from . import device as D
-from .maxcut_tfim import maxcut_tfim
+from .maxcut_tfim import _maxcut_tfim, maxcut_tfim  # noqa: F401
 from .util import HEURISTIC_THRESHOLD, as_matrix, get_cut, parse_best_guess
 
 
@@ -171,6 +171,16 @@ def spin_glass_solver(
     bp_damping=0.5,
 ):
     nodes, G_m = as_matrix(G)
+    return _spin_glass_solver(nodes, G_m, quality, shots, best_guess, is_maxcut_gpu, is_spin_glass, anneal_t,
+                              anneal_h, repulsion_base, gray_iterations, gray_seed_multiple, bp_scale, bp_damping)
+
+
+def _spin_glass_solver(nodes, G_m, quality, shots, best_guess, is_maxcut_gpu, is_spin_glass, anneal_t, anneal_h,
+                       repulsion_base, gray_iterations, gray_seed_multiple, bp_scale, bp_damping,
+                       threshold=HEURISTIC_THRESHOLD, jz_matrix=None):
+    """spin_glass_solver on a dense symmetric matrix; `threshold` and
+    `jz_matrix` as in maxcut_tfim._maxcut_tfim (the sparse entry point's
+    values differ)."""
     n_qubits = len(nodes)
 
     if n_qubits < 3:
@@ -184,24 +194,17 @@ def spin_glass_solver(
                 return "00", 0, (nodes, []), weight
             return "01", weight, ([nodes[0]], [nodes[1]]), -weight
 
-    if n_qubits < HEURISTIC_THRESHOLD:
+    if n_qubits < threshold:
         best_guess = None
 
     theta = parse_best_guess(best_guess, n_qubits)
     cut_value = None
     if theta is None:
-        bitstring, cut_value, _ = maxcut_tfim(
-            G_m,
-            quality=quality,
-            shots=shots,
-            is_spin_glass=is_spin_glass,
-            anneal_t=anneal_t,
-            anneal_h=anneal_h,
-            repulsion_base=repulsion_base,
-            is_maxcut_gpu=is_maxcut_gpu,
-            is_nested=True,
+        bitstring, cut_value, _ = _maxcut_tfim(
+            list(range(n_qubits)), G_m, quality, shots, is_spin_glass, anneal_t, anneal_h, repulsion_base,
+            threshold=threshold, jz_matrix=jz_matrix,
         )
-        if bp_scale is not None and n_qubits >= HEURISTIC_THRESHOLD:
+        if bp_scale is not None and n_qubits >= threshold:
             # keep whichever of the BP partition and the sample scores higher
             # (spin_glass_solver.py:493-523)
             bp_theta = bp_warm_start_dense(G_m, n_qubits, bp_scale, bp_damping)
@@ -226,7 +229,7 @@ def spin_glass_solver(
     else:
         max_energy = cut_value
 
-    if n_qubits < HEURISTIC_THRESHOLD:
+    if n_qubits < threshold:
         bitstring, l, r = get_cut(theta, nodes)
         if is_spin_glass:
             cut_value = float(cut0.item())

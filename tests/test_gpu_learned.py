@@ -113,3 +113,32 @@ def test_trained_proposals_beat_uniform_kicks():
     print("mean-best gain per held-out graph:", [round(g, 2) for g in gains])
     assert sum(g > 0 for g in gains) >= 5
     assert sum(gains) > 0
+
+
+@pytest.mark.parametrize("n", [100, 300, 1030])
+def test_tensor_core_messages_match_cuda_core_messages(n):
+    """The tcgen05 message products (A_hat X, forward and backward) give the
+    CUDA-core GEMM's logits and gradients to float32-accumulation accuracy,
+    on sizes that are not multiples of the 128-row tile or the 64-wide K step."""
+    from pyqrackising_b200 import learned as L
+    from pyqrackising_b200 import workloads as wl
+    from pyqrackising_b200.device import DeviceGraph
+
+    dg = DeviceGraph(wl.gnp_weighted(n, 0.1, seed=n, dist="normal"))
+    ctx = L.GraphContext(dg)
+    words = dg.pack(np.random.default_rng(n).random(n) < 0.5)
+    F = ctx.features(words)
+    tgt = torch.full((n,), 1.0 / n, dtype=torch.float32, device="cuda")
+    out = {}
+    for tcore in (False, True):
+        net = L.ProposalNet(seed=1)
+        net.tensor_cores = tcore
+        logits, cache = net.forward(ctx, F)
+        _, dl, _ = net.loss_grad(logits, tgt)
+        net.zero_grad()
+        net.backward(ctx, cache, dl)
+        out[tcore] = (logits.cpu().numpy().astype(np.float64), net.g.cpu().numpy().astype(np.float64))
+    (l0, g0), (l1, g1) = out[False], out[True]
+    assert np.abs(l1 - l0).max() <= 2e-2 * (np.abs(l0).max() + 1e-6)
+    cos = g0 @ g1 / (np.linalg.norm(g0) * np.linalg.norm(g1))
+    assert cos > 0.999
