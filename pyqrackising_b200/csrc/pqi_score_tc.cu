@@ -387,31 +387,17 @@ __device__ __forceinline__ void expand_word(uint32_t bits, T* __restrict__ dst) 
 }
 
 // Packed candidates -> the +-1 A operand (int8, or bf16 for the float path),
-// row pitch ld elements; each thread expands four words (one 16-byte load when
-// the rows are 16-byte aligned) into 128 contiguous int8 (256 bf16) outputs.
-// Columns at and beyond n are never read (the A tensor map ends at n).
+// row pitch ld elements: one word per thread, so a warp's stores cover
+// contiguous 32-byte (int8) or 64-byte (bf16) pieces of a row. Columns at and
+// beyond n are never read (the A tensor map ends at n).
 template <typename T>
 __global__ void expand_pm1_kernel(const uint32_t* __restrict__ theta, int shots, int n32, int ld,
                                   T* __restrict__ X) {
-  const int q32 = (n32 + 3) >> 2;  // word quads per row
-  const bool vec = (n32 & 3) == 0;
-  const long long total = (long long)shots * q32;
+  const long long total = (long long)shots * n32;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
-    const int b = (int)(e / q32), w0 = 4 * (int)(e - (long long)b * q32);
-    const uint32_t* src = theta + (size_t)b * n32 + w0;
-    T* dst = X + (size_t)b * ld + (size_t)w0 * 32;
-    if (vec) {
-      const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
-      expand_word<T>(v.x, dst);
-      expand_word<T>(v.y, dst + 32);
-      expand_word<T>(v.z, dst + 64);
-      expand_word<T>(v.w, dst + 96);
-    } else {
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if (w0 + i < n32) expand_word<T>(__ldg(src + i), dst + 32 * i);
-    }
+    const int b = (int)(e / n32), w = (int)(e - (long long)b * n32);
+    expand_word<T>(__ldg(theta + e), X + (size_t)b * ld + (size_t)w * 32);
   }
 }
 
@@ -538,8 +524,8 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     attr_set[i8] = true;
   }
   PQI_TRY(cudaMemsetAsync(ctl, 0, ctl_bytes, s));
-  const long long quads = (long long)shots * ((n32 + 3) / 4);
-  const int eg = (int)std::max<long long>(1, std::min<long long>((quads + 255) / 256, 148 * 16));
+  const long long words = (long long)shots * n32;
+  const int eg = (int)std::max<long long>(1, std::min<long long>((words + 255) / 256, 148 * 16));
   if (i8) {
     tc::expand_pm1_kernel<int8_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (int8_t*)X);
   } else {
