@@ -208,8 +208,13 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
     uint32_t* best_bits = best_states + (size_t)task * words_pitch;
     for (int w = threadIdx.x; w < n32; w += blockDim.x) c.bits[w] = init_states[(size_t)task * words_pitch + w];
     __syncthreads();
-    // 1. gains of the starting state, one warp per row
-    {
+    // 1. local fields of the starting state, y_v = sum_u x_u W_uv (W is
+    // symmetric). Below 2048 nodes a warp per row (row dot product, shuffle
+    // reduction): more rows in flight per CTA. From 2048 nodes every row u adds
+    // +-W_u to each thread's own nodes (rows ascending, CH groups of four per
+    // pass in registers): a memory stream with few instructions, which leaves
+    // the SM to the flips of the other resident tasks.
+    if (n < 2048) {
       const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
       for (int k = threadIdx.x >> 5; k < n; k += warps) {
         const WT* row = c.W + (size_t)k * c.ld;
@@ -219,7 +224,46 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
           acc += ((c.bits[v >> 5] >> (v & 31)) & 1) ? w : -w;
         }
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
-        if (lane == 0) c.g[fpos(k)] = acc;  // local field y_k
+        if (lane == 0) c.g[fpos(k)] = acc;
+      }
+    } else {
+      for (int base = 4 * threadIdx.x; base < n; base += CH * 1024) {
+        GT acc[4 * CH];
+#pragma unroll
+        for (int e = 0; e < 4 * CH; ++e) acc[e] = 0;
+#pragma unroll 2
+        for (int u = 0; u < n; ++u) {
+          const WT* __restrict__ row = c.W + (size_t)u * c.ld;
+          const bool xu = (c.bits[u >> 5] >> (u & 31)) & 1u;
+#pragma unroll
+          for (int j = 0; j < CH; ++j) {
+            const int v = base + j * 1024;
+            if (v < n) {
+              WT w4[4];
+              if (v + 3 < n) {
+                if constexpr (sizeof(WT) == 4) {
+                  const float4 t = __ldg(reinterpret_cast<const float4*>(row + v));
+                  w4[0] = t.x; w4[1] = t.y; w4[2] = t.z; w4[3] = t.w;
+                } else {
+                  const char4 t = __ldg(reinterpret_cast<const char4*>(row + v));
+                  w4[0] = t.x; w4[1] = t.y; w4[2] = t.z; w4[3] = t.w;
+                }
+              } else {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) w4[i] = (v + i < n) ? __ldg(row + v + i) : (WT)0;
+              }
+#pragma unroll
+              for (int i = 0; i < 4; ++i) acc[4 * j + i] += xu ? (GT)w4[i] : -(GT)w4[i];
+            }
+          }
+        }
+#pragma unroll
+        for (int j = 0; j < CH; ++j)
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const int v = base + j * 1024 + i;
+            if (v < n) c.g[fpos(v)] = acc[4 * j + i];
+          }
       }
     }
     __syncthreads();
