@@ -433,7 +433,7 @@ def batched_leg(graphs=512, seeds=256):
     }
 
 
-def flip_bandwidth_leg(n=8192, tasks=1776):
+def flip_bandwidth_leg(n=8192, tasks=1776, fields="f64"):
     """Flip updates on the SK spin glass (W = 256 MB float32, larger than L2):
     many starts of the batched ascent at once; each accepted flip reads one W
     row (n * 4 bytes) and updates the task's n local fields."""
@@ -447,18 +447,18 @@ def flip_bandwidth_leg(n=8192, tasks=1776):
     bs = BatchedSearch([dg])
     tg = torch.zeros(tasks, dtype=torch.int32, device=dg.device)
     w0 = bs.random_states(np.zeros(tasks, dtype=np.int32), seed=5)
-    bs.run(tg, w0, True, rounds=0, flip_budget=64)  # warm
+    bs.run(tg, w0, True, rounds=0, flip_budget=64, fields=fields)  # warm
     torch.cuda.synchronize()
     # starting fields cost n rows per task: time them alone (zero-flip budget
     # is not allowed, so a one-flip budget) and subtract
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
-    _, _, f1, _ = bs.run(tg, w0, True, rounds=0, flip_budget=1)
+    _, _, f1, _ = bs.run(tg, w0, True, rounds=0, flip_budget=1, fields=fields)
     b.record()
     b.synchronize()
     t_init = a.elapsed_time(b)
     a.record()
-    _, _, f2, st = bs.run(tg, w0, True, rounds=0, flip_budget=1 + 256)
+    _, _, f2, st = bs.run(tg, w0, True, rounds=0, flip_budget=1 + 256, fields=fields)
     b.record()
     b.synchronize()
     t_all = a.elapsed_time(b)
@@ -467,7 +467,7 @@ def flip_bandwidth_leg(n=8192, tasks=1776):
     hbm, _, src = peaks()
     gbs = flips * n * 4 / dt / 1e9
     return {
-        "workload": f"SK n={n} float32, {tasks} starts of the batched ascent, 256 flips each after the starting fields",
+        "workload": f"SK n={n} float32, {tasks} starts of the batched ascent, 256 flips each after the starting fields, {fields} local fields",
         "flips": flips,
         "flips_per_s": flips / dt,
         "row_bytes_per_flip": n * 4,
@@ -632,6 +632,7 @@ def main():
             line["batched"] = batched_leg()
             line["learned"] = learned_leg()
             line["flip_updates"] = flip_bandwidth_leg()
+            line["flip_updates_f32_fields"] = flip_bandwidth_leg(fields="f32")
         if world == 1:
             try:
                 line["cpu_baseline"] = cpu_baseline(W, make_batch(0))

@@ -313,6 +313,23 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
                             unsigned long long* flips_total, int* status, void* stream);
 
 /*
+ * pqi_batch_search with float32 local fields for float-weight graphs (int8
+ * graphs are unchanged: their fields are exact int32). Half the shared memory
+ * and fewer registers per task, so four tasks are resident per SM instead of
+ * three; the gains are float32 (as the reference's), the running value and the
+ * returned values stay float64 sums of exact-to-float32 gains. Field rounding
+ * can change the trajectory against the float64-field form. No reference
+ * counterpart.
+ */
+pqi_status pqi_batch_search_f32(const void* graphs, int num_graphs, const int* task_graph,
+                                const uint32_t* init_states, int words_pitch, int tasks,
+                                int max_n, int kind, int is_spin_glass, int rounds, int kick,
+                                int flip_budget, uint64_t seed, const double* kick_cdf,
+                                const long long* cdf_offset, uint32_t* best_states,
+                                double* best_values, unsigned long long* flips_total,
+                                int* status, void* stream);
+
+/*
  * pqi_batch_search with one warp per task instead of one CTA: the same search,
  * selection rule, kick stream, outputs and status, for graphs with
  * max_n <= 1024. Fields and bits live in registers (no shared memory, no

@@ -75,10 +75,13 @@ class BatchedSearch:
 
     def run(self, task_graph, init_words: torch.Tensor, is_spin_glass: bool, rounds: int = 0, kick: int = 4,
             seed: int = 0, kick_cdf: torch.Tensor | None = None, cdf_offset: torch.Tensor | None = None,
-            flip_budget: int | None = None, variant: str = "cta", warps_per_sm: int = 0, out=None):
+            flip_budget: int | None = None, variant: str = "cta", warps_per_sm: int = 0, out=None,
+            fields: str = "f64"):
         """Iterated local search of every task. variant: "cta" (one CTA per
         task, any n) or "warp" (one warp per task, max_n <= 1024); both give
-        the same results. `out` = (best_states, best_values, flips, status)
+        the same results. fields: "f64" (default) or "f32" (CTA form, float
+        graphs: float32 local fields, more resident tasks per SM; rounding can
+        change trajectories). `out` = (best_states, best_values, flips, status)
         device buffers to fill (for CUDA-graph capture); flips and status are
         accumulated into, so zero them between uses."""
         tg = task_graph if torch.is_tensor(task_graph) else torch.as_tensor(np.asarray(task_graph, dtype=np.int32)).to(self.device)
@@ -102,8 +105,10 @@ class BatchedSearch:
             return best_values, best_states.view(tasks, self.pitch), flips, status
         if variant != "cta":
             raise ValueError("variant must be 'cta' or 'warp'")
+        if fields not in ("f64", "f32"):
+            raise ValueError("fields must be 'f64' or 'f32'")
         _lib.call(
-            "pqi_batch_search",
+            "pqi_batch_search_f32" if fields == "f32" else "pqi_batch_search",
             D._ptr(self.desc),
             len(self.graphs),
             D._ptr(tg),

@@ -181,15 +181,19 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   *out_key = gk;
 }
 
-template <typename WT, int CH>
-__global__ void __launch_bounds__(256, 3) batch_search_kernel(
+// F32: float graphs keep float32 local fields (half the shared memory and
+// fewer registers, so more resident tasks per SM); gains, the selection rule
+// and the float64 running value are unchanged in form.
+template <typename WT, int CH, bool F32>
+__global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
     const BatchGraph* __restrict__ graphs, const int* __restrict__ task_graph,
     const uint32_t* __restrict__ init_states, int words_pitch, int tasks, int spin, int rounds,
     int kick, int flip_budget, uint64_t seed, const double* __restrict__ kick_cdf,
     const long long* __restrict__ cdf_offset, uint32_t* __restrict__ best_states,
     double* __restrict__ best_values, unsigned long long* __restrict__ flips_total,
     int* __restrict__ status) {
-  typedef typename std::conditional<sizeof(WT) == 1, int, double>::type GT;
+  typedef typename std::conditional<
+      sizeof(WT) == 1, int, typename std::conditional<F32, float, double>::type>::type GT;
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[32];
   __shared__ unsigned long long red_key[2][8];
@@ -227,16 +231,19 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
         if (lane == 0) c.g[fpos(k)] = acc;
       }
     } else {
-      for (int base = 4 * threadIdx.x; base < n; base += CH * 1024) {
-        GT acc[4 * CH];
+      // at most two groups per pass: eight accumulators keep the register
+      // budget of three resident CTAs per SM
+      constexpr int CI = CH > 2 ? 2 : CH;
+      for (int base = 4 * threadIdx.x; base < n; base += CI * 1024) {
+        GT acc[4 * CI];
 #pragma unroll
-        for (int e = 0; e < 4 * CH; ++e) acc[e] = 0;
+        for (int e = 0; e < 4 * CI; ++e) acc[e] = 0;
 #pragma unroll 2
         for (int u = 0; u < n; ++u) {
           const WT* __restrict__ row = c.W + (size_t)u * c.ld;
           const bool xu = (c.bits[u >> 5] >> (u & 31)) & 1u;
 #pragma unroll
-          for (int j = 0; j < CH; ++j) {
+          for (int j = 0; j < CI; ++j) {
             const int v = base + j * 1024;
             if (v < n) {
               WT w4[4];
@@ -258,7 +265,7 @@ __global__ void __launch_bounds__(256, 3) batch_search_kernel(
           }
         }
 #pragma unroll
-        for (int j = 0; j < CH; ++j)
+        for (int j = 0; j < CI; ++j)
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int v = base + j * 1024 + i;
@@ -550,12 +557,15 @@ extern "C" {
 
 size_t pqi_batch_graph_desc_bytes(void) { return sizeof(BatchGraph); }
 
-pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_graph,
-                            const uint32_t* init_states, int words_pitch, int tasks, int max_n,
-                            int kind, int is_spin_glass, int rounds, int kick, int flip_budget,
-                            uint64_t seed, const double* kick_cdf, const long long* cdf_offset,
-                            uint32_t* best_states, double* best_values,
-                            unsigned long long* flips_total, int* status, void* stream) {
+}  // extern "C"
+
+static pqi_status batch_search_impl(const void* graphs, int num_graphs, const int* task_graph,
+                                    const uint32_t* init_states, int words_pitch, int tasks,
+                                    int max_n, int kind, int is_spin_glass, int rounds, int kick,
+                                    int flip_budget, uint64_t seed, const double* kick_cdf,
+                                    const long long* cdf_offset, uint32_t* best_states,
+                                    double* best_values, unsigned long long* flips_total,
+                                    int* status, void* stream, bool f32) {
   PQI_CHECK_ARG(graphs && num_graphs > 0 && task_graph && init_states && tasks > 0 && max_n > 0);
   PQI_CHECK_ARG(best_states && best_values && flips_total && status && rounds >= 0 && kick >= 0);
   PQI_CHECK_ARG(words_pitch >= (max_n + 31) / 32 && flip_budget > 0);
@@ -563,7 +573,8 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
   cudaStream_t s = as_stream(stream);
   const bool i8 = kind == PQI_W_I8;
   const size_t smem = (((size_t)((max_n + 31) >> 5) * 4 + 15) & ~size_t(15)) +
-                      (size_t)((max_n + 1023) / 1024 * 1024) * (i8 ? sizeof(int) : sizeof(double)) +
+                      (size_t)((max_n + 1023) / 1024 * 1024) *
+                          (i8 ? sizeof(int) : (f32 ? sizeof(float) : sizeof(double))) +
                       (size_t)((max_n + 31) >> 5) * 4;  // kicked set of the current round
   PQI_CHECK_ARG(smem <= 200 * 1024);
   static int num_sms = 0;
@@ -579,16 +590,16 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
   // (the whole row for n <= 4 * 256 * CH). CH = 4 keeps three CTAs per SM
   // within the register file (8 groups spill at that occupancy and run slower
   // on SK n = 8192 than two chunks of 4).
-#define PQI_BATCH_LAUNCH(WT_, CH_)                                                              \
+#define PQI_BATCH_LAUNCH(WT_, CH_, F_)                                                          \
   do {                                                                                         \
-    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_>,                               \
+    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_>,                               \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
-    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_>,                               \
+    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_>,                               \
                                  cudaFuncAttributePreferredSharedMemoryCarveout, 100));        \
-    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel<WT_, CH_>, \
+    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel<WT_, CH_, F_>, \
                                                           256, smem));                         \
     const int grid = std::max(1, std::min(tasks, num_sms * std::max(1, per_sm)));             \
-    batch_search_kernel<WT_, CH_><<<grid, 256, smem, s>>>(                                     \
+    batch_search_kernel<WT_, CH_, F_><<<grid, 256, smem, s>>>(                                     \
         gd, task_graph, init_states, words_pitch, tasks, is_spin_glass, rounds, kick,          \
         flip_budget, seed, kick_cdf, cdf_offset, best_states, best_values, flips_total,        \
         status);                                                                               \
@@ -596,20 +607,53 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
   const int groups = (max_n + 1023) / 1024;  // groups of four per thread
   if (i8) {
     if (groups <= 2) {
-      PQI_BATCH_LAUNCH(int8_t, 2);
+      PQI_BATCH_LAUNCH(int8_t, 2, false);
     } else {
-      PQI_BATCH_LAUNCH(int8_t, 4);
+      PQI_BATCH_LAUNCH(int8_t, 4, false);
+    }
+  } else if (f32) {
+    if (groups <= 2) {
+      PQI_BATCH_LAUNCH(float, 2, true);
+    } else {
+      PQI_BATCH_LAUNCH(float, 4, true);
     }
   } else {
     if (groups <= 2) {
-      PQI_BATCH_LAUNCH(float, 2);
+      PQI_BATCH_LAUNCH(float, 2, false);
     } else {
-      PQI_BATCH_LAUNCH(float, 4);
+      PQI_BATCH_LAUNCH(float, 4, false);
     }
   }
 #undef PQI_BATCH_LAUNCH
   PQI_LAUNCHED("batch_search_kernel");
   return PQI_OK;
+}
+
+extern "C" {
+
+pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_graph,
+                            const uint32_t* init_states, int words_pitch, int tasks, int max_n,
+                            int kind, int is_spin_glass, int rounds, int kick, int flip_budget,
+                            uint64_t seed, const double* kick_cdf, const long long* cdf_offset,
+                            uint32_t* best_states, double* best_values,
+                            unsigned long long* flips_total, int* status, void* stream) {
+  return batch_search_impl(graphs, num_graphs, task_graph, init_states, words_pitch, tasks, max_n,
+                           kind, is_spin_glass, rounds, kick, flip_budget, seed, kick_cdf,
+                           cdf_offset, best_states, best_values, flips_total, status, stream,
+                           false);
+}
+
+pqi_status pqi_batch_search_f32(const void* graphs, int num_graphs, const int* task_graph,
+                                const uint32_t* init_states, int words_pitch, int tasks,
+                                int max_n, int kind, int is_spin_glass, int rounds, int kick,
+                                int flip_budget, uint64_t seed, const double* kick_cdf,
+                                const long long* cdf_offset, uint32_t* best_states,
+                                double* best_values, unsigned long long* flips_total,
+                                int* status, void* stream) {
+  return batch_search_impl(graphs, num_graphs, task_graph, init_states, words_pitch, tasks, max_n,
+                           kind, is_spin_glass, rounds, kick, flip_budget, seed, kick_cdf,
+                           cdf_offset, best_states, best_values, flips_total, status, stream,
+                           true);
 }
 
 pqi_status pqi_batch_search_warp(const void* graphs, int num_graphs, const int* task_graph,

@@ -213,3 +213,33 @@ def test_batched_solver_mixed_kinds_graph_capture(oracle_mod):
     form, wps = grp["form"]
     v2, _, _, _ = grp["bs"].run(grp["tg"], grp["init"], True, rounds=2, kick=6, seed=5, variant=form, warps_per_sm=wps)
     assert torch.allclose(v2, grp["out"][1], rtol=0, atol=0)
+
+
+@pytest.mark.parametrize("kind", ["int", "float"])
+def test_float32_fields_form(kind, oracle_mod):
+    """fields="f32": int8 graphs are unchanged (exact int32 fields); float
+    graphs end at local optima whose returned values match float64
+    re-scoring within float32-gain accuracy."""
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    O = oracle_mod
+    Ws = _graphs(kind, [100, 257, 1000, 2500], seed=8)
+    bs = BatchedSearch([DeviceGraph(W) for W in Ws])
+    task_graph = [0, 1, 2, 3, 3, 2]
+    words = bs.random_states(task_graph, seed=4)
+    v64, b64, f64, _ = bs.run(task_graph, words, True, rounds=2, kick=6, seed=3)
+    v32, b32, f32, st = bs.run(task_graph, words, True, rounds=2, kick=6, seed=3, fields="f32")
+    assert int(st.item()) == 0
+    if kind == "int":
+        assert torch.equal(b32, b64) and torch.equal(v32, v64)
+        return
+    for t, g in enumerate(task_graph):
+        bits = bs.unpack(b32, task_graph)[t]
+        W = Ws[g]
+        e = O.compute_energy(bits, W)
+        assert float(v32[t]) == pytest.approx(e, rel=1e-5, abs=1e-5 * np.abs(W).sum())
+        x = np.where(bits, 1.0, -1.0)
+        Wd = W.astype(np.float64).copy()
+        np.fill_diagonal(Wd, 0.0)
+        assert np.all(x * (Wd @ x) <= 1e-5 * np.abs(Wd).sum(axis=1).max())
