@@ -379,7 +379,7 @@ def learned_leg():
     """Config 5: the committed trained proposal network on G(16384, 0.01) with
     N(0, 1) weights: the batched iterated search with uniform kicks and with
     the network's per-task proposals from the same optima, each refined by the
-    plain local search (the judge), next to the plain search alone."""
+    plain local search (the arbiter), next to the plain search alone."""
     from pyqrackising_b200 import learned as L
     from pyqrackising_b200.train_proposals import evaluate
 

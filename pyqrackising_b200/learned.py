@@ -16,7 +16,7 @@ led somewhere better). At inference each task gets the proposal of its own
 local optimum, flattened by a temperature (``task_proposals``), as the kick
 distribution of the batched search (``BatchedSearch.run(kick_cdf=...)``, one
 graph descriptor per task); kicks are drawn without replacement within a round. The plain search stays
-both the judge (every returned value comes from the search's own exact
+both the arbiter (every returned value comes from the search's own exact
 bookkeeping and float64 re-scoring) and the fallback (uniform kicks).
 """
 

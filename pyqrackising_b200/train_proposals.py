@@ -10,7 +10,7 @@ differs), the network takes one Adam pass over them, and the chunk is dropped.
 Evaluation: one graph (default G(16384, 0.01) with N(0, 1) weights); from the
 same starting states, the batched iterated search with uniform kicks and with
 kicks drawn from the network's proposal, next to the plain local search of
-``spin_glass_solver`` (the fallback and the judge: every value is the
+``spin_glass_solver`` (the fallback and the arbiter: every value is the
 search's exact bookkeeping, re-scored in float64).
 
     python -m pyqrackising_b200.train_proposals --graphs 10000 --out net.pt
@@ -135,7 +135,7 @@ def evaluate(net: L.ProposalNet | None, n: int = 16384, p: float = 0.01, seed: i
              starts: int = 32, rounds: int = 8):
     """The evaluation graph. The batched iterated search runs with uniform and
     with proposal kicks from the same ascent optima; the plain local search of
-    spin_glass_solver is the judge and the refiner: it runs from a random start
+    spin_glass_solver is the arbiter and the refiner: it runs from a random start
     and from each search's best state, and every value is float64 re-scoring."""
     SG = importlib.import_module("pyqrackising_b200.spin_glass_solver")
     W = wl.gnp_weighted(n, p, seed=seed, dist="normal")

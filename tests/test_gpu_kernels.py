@@ -4,7 +4,7 @@ code) and against the oracle on fresh inputs.
 
 Tolerances: integer weights must match bit for bit (values and selected
 indices). Float weights: values within 1e-5 relative to the row's absolute sum
-(gains) or to the sum of |W| (cuts), the north-star bound for float32 inputs;
+(gains) or to the sum of |W| (cuts), the stated bound for float32 inputs;
 the reference itself sums in float32, so its own error is of that order.
 """
 
