@@ -118,7 +118,9 @@ pqi_status pqi_prepare_weights(const float* W, int n, const pqi_weight_stats* st
                                pqi_weights* out_host, void* stream);
 
 /* Select the batched-scoring implementation: 0 = tensor cores (tcgen05, the
- * default), 1 = CUDA cores. Process-wide; used to cross-check the two. */
+ * default; CTA pairs with cta_group::2 MMAs for batches of more than 128
+ * candidates), 1 = CUDA cores, 2 = tensor cores with single-CTA MMAs.
+ * Process-wide; used to cross-check the implementations. */
 pqi_status pqi_score_set_path(int path);
 
 /* Record two caller-owned cudaEvent_t on the call's stream immediately before

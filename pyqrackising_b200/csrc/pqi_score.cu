@@ -148,8 +148,9 @@ pqi_status score_simt(const pqi_weights* w, const uint32_t* theta, int shots, do
   return PQI_OK;
 }
 
-// Set by pqi_score_set_path: 0 = automatic (tensor cores when available),
-// 1 = CUDA cores only. Used by tests to compare the two paths.
+// Set by pqi_score_set_path: 0 = automatic (tensor cores when available, CTA
+// pairs for batches of more than 128 candidates), 1 = CUDA cores only,
+// 2 = tensor cores without CTA pairs. Used by tests to compare the paths.
 int g_score_path = 0;
 
 pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int spin,
@@ -170,7 +171,7 @@ using namespace pqi;
 extern "C" {
 
 pqi_status pqi_score_set_path(int path) {
-  if (path < 0 || path > 1) return PQI_EINVAL;
+  if (path < 0 || path > 2) return PQI_EINVAL;
   g_score_path = path;
   return PQI_OK;
 }
@@ -198,7 +199,7 @@ pqi_status pqi_calculate_cut(const pqi_weights* w, const uint32_t* theta, int sh
   Workspace ws(workspace, workspace_bytes);
   unsigned long long* key = ws.take<unsigned long long>(1);
   PQI_CHECK_ARG(key);
-  if (g_score_path == 0) {
+  if (g_score_path != 1) {
     pqi_status rc = score_tc(w, theta, shots, is_spin_glass, geo, energies, best_energy,
                              best_index, ws, s);
     if (rc != PQI_ENOTSUP) return rc;

@@ -26,6 +26,8 @@
 
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "pqi_common.cuh"
 #include "pqi_tc.cuh"
 
@@ -41,6 +43,15 @@ constexpr int A_STAGE = BM * BK_BYTES;   // 16 KB
 constexpr int B_STAGE = BN * BK_BYTES;   // 32 KB
 constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;  // + alignment slack
+// CTA-pair mode (cta_group::2): a pair computes 256 candidates x 256 nodes
+// with M = 256 MMAs issued by the even CTA; each CTA loads its 128 candidate
+// rows and half (128 rows) of the W tile, so each CTA's W traffic halves.
+constexpr int B_STAGE_PAIR = (BN / 2) * BK_BYTES;  // 16 KB
+constexpr int STAGE_BYTES_PAIR = A_STAGE + B_STAGE_PAIR;
+constexpr int STAGES_PAIR = 6;
+constexpr int MAX_STAGES = STAGES_PAIR;
+static_assert(STAGES_PAIR * STAGE_BYTES_PAIR + 1024 <= SMEM_BYTES, "pair ring fits the same smem");
+constexpr uint32_t kPeerMask = 0xFEFFFFFFu;  // clears the pair bit of a shared::cluster address
 
 // Instruction descriptors (M = 128, N = 256, both operands K-major).
 constexpr uint32_t kIdescI8 = (2u << 4)      // D: s32
@@ -51,6 +62,9 @@ constexpr uint32_t kIdescBF16 = (1u << 4)    // D: f32
                                 | (1u << 7)  // A: bf16
                                 | (1u << 10) // B: bf16
                                 | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+constexpr uint32_t kIdescI8Pair = (kIdescI8 & ~(0x1Fu << 24)) | ((uint32_t)(256 >> 4) << 24);
+constexpr uint32_t kIdescBF16Pair = (kIdescBF16 & ~(0x1Fu << 24)) | ((uint32_t)(256 >> 4) << 24);
 
 // Warp roles of the persistent kernel (6 warps).
 constexpr int TMA_WARP = 0;       // warp 0 lane 0: TMA loads of the X and W tiles
@@ -67,7 +81,7 @@ __device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 128;" 
 // split between two CTAs goes through per-tile partials summed in tile order
 // by the CTA that completes it. The finisher converts q to the reference's
 // value and folds it into the selection key; the last block decodes it.
-template <bool kInt8>
+template <bool kInt8, bool PAIR>
 __global__ void __launch_bounds__(PTHREADS, 1)
     score_tc_kernel(const __grid_constant__ CUtensorMap map_a,
                     const __grid_constant__ CUtensorMap map_b0,
@@ -78,8 +92,8 @@ __global__ void __launch_bounds__(PTHREADS, 1)
                     unsigned long long* __restrict__ key, float* __restrict__ best_energy,
                     int* __restrict__ best_index, int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[STAGES];
-  __shared__ __align__(8) uint64_t empty_bar[STAGES];
+  __shared__ __align__(8) uint64_t full_bar[MAX_STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[MAX_STAGES];
   __shared__ __align__(8) uint64_t accf_bar[2];
   __shared__ __align__(8) uint64_t acce_bar[2];
   __shared__ uint32_t tmem_base_holder;
@@ -90,37 +104,58 @@ __global__ void __launch_bounds__(PTHREADS, 1)
   const uint32_t raw = smem_u32(smem_raw);
   uint8_t* smem = smem_raw + ((1024 - (raw & 1023)) & 1023);
 
+  // pair mode: ranks 0 (issues the MMAs) and 1 of a 2-CTA cluster; a unit of
+  // work is the pair, a tile covers 256 candidates (128 per CTA)
+  constexpr int NST = PAIR ? STAGES_PAIR : STAGES;
+  constexpr int SB = PAIR ? STAGE_BYTES_PAIR : STAGE_BYTES;
+  constexpr int UM = PAIR ? 2 * BM : BM;  // candidates per tile
+  const int rank = PAIR ? (int)(blockIdx.x & 1) : 0;
+  const int unit = PAIR ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
+  const int units = PAIR ? (int)(gridDim.x >> 1) : (int)gridDim.x;
   const int ntn = (n + BN - 1) / BN;
-  const int ntm = (shots + BM - 1) / BM;
-  const int ntiles = ntn * ntm;
-  // each CTA walks one contiguous chunk of tiles (candidate-block major), so
-  // most blocks are finished by one CTA with q kept in registers
-  const int t_begin = (int)(((long long)blockIdx.x * ntiles) / gridDim.x);
-  const int t_end = (int)(((long long)(blockIdx.x + 1) * ntiles) / gridDim.x);
+  const int ntm = (shots + BM - 1) / BM;       // 128-candidate blocks (finish bookkeeping)
+  const int ntu = (shots + UM - 1) / UM;       // tile rows
+  const int ntiles = ntn * ntu;
+  // each unit walks one contiguous chunk of tiles (candidate-block major), so
+  // most blocks are finished by one unit with q kept in registers
+  const int t_begin = (int)(((long long)unit * ntiles) / units);
+  const int t_end = (int)(((long long)(unit + 1) * ntiles) / units);
   const int kb_per_pass = kInt8 ? (n + BK_BYTES - 1) / BK_BYTES : (n + 63) / 64;
   const int kblocks = kInt8 ? kb_per_pass : 2 * kb_per_pass;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < NST; ++s) {
       mbar_init(&full_bar[s], 1);
       mbar_init(&empty_bar[s], 1);
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(&accf_bar[a], 1);
-      mbar_init(&acce_bar[a], 4);
+      mbar_init(&acce_bar[a], PAIR ? 8 : 4);  // pair: both CTAs' epilogue warps
     }
     s_fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == MMA_WARP) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                     smem_u32(&tmem_base_holder)),
-                 "r"(ACC_COLS));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    if constexpr (PAIR) {
+      // both CTAs' warp 1, same destination: the pair's TMEM columns
+      asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       smem_u32(&tmem_base_holder)),
+                   "r"(ACC_COLS));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+    } else {
+      asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                       smem_u32(&tmem_base_holder)),
+                   "r"(ACC_COLS));
+      asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
+  if constexpr (PAIR) {
+    cooperative_groups::this_cluster().sync();  // both CTAs' barriers initialised
+  } else {
+    __syncthreads();
+  }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem_base = tmem_base_holder;
 
@@ -129,27 +164,36 @@ __global__ void __launch_bounds__(PTHREADS, 1)
       uint32_t it = 0;
       bool ok = true;
       for (int t = t_begin; t < t_end && ok; ++t) {
-        const int m0 = (t / ntn) * BM, n0 = (t % ntn) * BN;
+        const int m0 = (t / ntn) * UM + rank * BM, n0 = (t % ntn) * BN + rank * (BN / 2);
         for (int kb = 0; kb < kblocks; ++kb, ++it) {
-          const int s = it % STAGES;
-          if (it >= STAGES && !mbar_wait(&empty_bar[s], ((it / STAGES) - 1) & 1)) {
+          const int s = it % NST;
+          if (it >= NST && !mbar_wait(&empty_bar[s], ((it / NST) - 1) & 1)) {
             ok = false;
             s_fail = 1;
             break;
           }
           const int kk = kInt8 ? kb * BK_BYTES : (kb % kb_per_pass) * 64;
           const CUtensorMap* mb = (kInt8 || kb < kb_per_pass) ? &map_b0 : &map_b1;
-          uint8_t* dst = smem + s * STAGE_BYTES;
-          mbar_expect_tx(&full_bar[s], STAGE_BYTES);
-          tma_load_2d(dst, &map_a, &full_bar[s], kk, m0);
-          tma_load_2d(dst + A_STAGE, mb, &full_bar[s], kk, n0);
+          uint8_t* dst = smem + s * SB;
+          if constexpr (PAIR) {
+            // both CTAs' bytes count on the even CTA's barrier, armed there
+            if (rank == 0) mbar_expect_tx(&full_bar[s], 2 * SB);
+            const uint32_t bar = smem_u32(&full_bar[s]) & kPeerMask;
+            tma_load_2d_pair(dst, &map_a, bar, kk, m0);
+            tma_load_2d_pair(dst + A_STAGE, mb, bar, kk, n0);
+          } else {
+            mbar_expect_tx(&full_bar[s], STAGE_BYTES);
+            tma_load_2d(dst, &map_a, &full_bar[s], kk, m0);
+            tma_load_2d(dst + A_STAGE, mb, &full_bar[s], kk, n0);
+          }
         }
       }
     }
     __syncwarp();
   } else if (warp == MMA_WARP) {
-    if (lane == 0) {
-      const uint32_t idesc = kInt8 ? kIdescI8 : kIdescBF16;
+    if (lane == 0 && rank == 0) {  // pair: the even CTA issues for both
+      const uint32_t idesc = PAIR ? (kInt8 ? kIdescI8Pair : kIdescBF16Pair)
+                                  : (kInt8 ? kIdescI8 : kIdescBF16);
       uint32_t it = 0;
       int i = 0;
       bool ok = true;
@@ -162,22 +206,38 @@ __global__ void __launch_bounds__(PTHREADS, 1)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tmem_d = tmem_base + (uint32_t)(a * BN);
         for (int kb = 0; kb < kblocks; ++kb, ++it) {
-          const int s = it % STAGES;
-          if (!mbar_wait(&full_bar[s], (it / STAGES) & 1)) {
+          const int s = it % NST;
+          if (!mbar_wait(&full_bar[s], (it / NST) & 1)) {
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
+          const uint32_t a_addr = smem_u32(smem + s * SB);
           const uint32_t b_addr = a_addr + A_STAGE;
 #pragma unroll
           for (int k = 0; k < BK_BYTES / 32; ++k) {
-            mma<kInt8>(tmem_d, sw128_desc(a_addr + k * 32), sw128_desc(b_addr + k * 32), idesc,
-                       (kb > 0 || k > 0) ? 1u : 0u);
+            if constexpr (PAIR) {
+              mma_pair<kInt8>(tmem_d, sw128_desc(a_addr + k * 32), sw128_desc(b_addr + k * 32),
+                              idesc, (kb > 0 || k > 0) ? 1u : 0u);
+            } else {
+              mma<kInt8>(tmem_d, sw128_desc(a_addr + k * 32), sw128_desc(b_addr + k * 32), idesc,
+                         (kb > 0 || k > 0) ? 1u : 0u);
+            }
           }
-          mma_commit(&empty_bar[s]);  // frees the stage once these MMAs have read it
+          // frees the stage (in both CTAs of a pair) once these MMAs have read it
+          if constexpr (PAIR) {
+            mma_commit_pair(&empty_bar[s]);
+          } else {
+            mma_commit(&empty_bar[s]);
+          }
         }
-        if (ok) mma_commit(&accf_bar[a]);  // accumulator a complete
+        if (ok) {  // accumulator a complete
+          if constexpr (PAIR) {
+            mma_commit_pair(&accf_bar[a]);
+          } else {
+            mma_commit(&accf_bar[a]);
+          }
+        }
       }
       if (!ok) s_fail = 1;
     }
@@ -192,8 +252,9 @@ __global__ void __launch_bounds__(PTHREADS, 1)
     int i = 0;
     for (int t = t_begin; t < t_end; ++t, ++i) {
       const int a = i & 1;
-      const int tm = t / ntn, tn = t % ntn;
-      const int b = tm * BM + row, n0 = tn * BN;
+      const int tm = t / ntn, tn = t % ntn;                // tile row, node tile
+      const int tm128 = tm * (PAIR ? 2 : 1) + rank;          // this CTA's 128-candidate block
+      const int b = tm128 * BM + row, n0 = tn * BN;
       // this CTA's share of candidate block tm: whole, or split with a neighbour
       const int blk0 = tm * ntn;
       const int first = max(t_begin, blk0), last = min(t_end, blk0 + ntn) - 1;
@@ -287,14 +348,20 @@ __global__ void __launch_bounds__(PTHREADS, 1)
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
-      if (lane == 0) mbar_arrive(&acce_bar[a]);  // accumulator a may be overwritten
+      if (lane == 0) {  // accumulator a may be overwritten
+        if (PAIR && rank == 1) {
+          mbar_arrive_remote0(&acce_bar[a]);  // the even CTA issues the MMAs
+        } else {
+          mbar_arrive(&acce_bar[a]);
+        }
+      }
       bool finish = false;  // this CTA folds block tm into the selection
       double q = 0.0;
       if (whole) {
         qacc_i += qt_i;
         qacc_f += qt_f;
         if (t == last) {
-          finish = true;
+          finish = tm128 < ntm;  // (a pair's odd half can lie wholly past the batch)
           q = kInt8 ? (double)qacc_i : qacc_f;
           qacc_i = 0;
           qacc_f = 0.0;
@@ -303,11 +370,11 @@ __global__ void __launch_bounds__(PTHREADS, 1)
         // split block: per-tile partials, summed in tile order by the CTA that
         // completes the block's tile count
         if (b < shots) qpart[(size_t)tn * shots + b] = kInt8 ? (double)qt_i : qt_f;
-        if (t == last) {
+        if (t == last && tm128 < ntm) {  // (a pair's odd half can lie wholly past the batch)
           __threadfence();
           epi_barrier();
           if (quarter == 0 && lane == 0)
-            s_bcast = atomicAdd(&mcount[tm], (unsigned)(last - first + 1)) +
+            s_bcast = atomicAdd(&mcount[tm128], (unsigned)(last - first + 1)) +
                       (unsigned)(last - first + 1);
           epi_barrier();
           if (s_bcast == (unsigned)ntn) {
@@ -351,10 +418,21 @@ __global__ void __launch_bounds__(PTHREADS, 1)
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  __syncthreads();
+  if constexpr (PAIR) {
+    // both CTAs done: no MMA writes the peer's TMEM, no arrival targets the
+    // even CTA's barriers, before either releases TMEM or exits
+    cooperative_groups::this_cluster().sync();
+  } else {
+    __syncthreads();
+  }
   if (warp == MMA_WARP) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
-                 "r"(ACC_COLS));
+    if constexpr (PAIR) {
+      asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                   "r"(ACC_COLS));
+    } else {
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                   "r"(ACC_COLS));
+    }
   }
   if (threadIdx.x == 0 && s_fail) atomicExch(err, 1);
 }
@@ -467,6 +545,7 @@ bool cached_map(CUtensorMap* out, const void* base, bool int8, int rows, int col
 
 extern cudaEvent_t g_score_ev_before, g_score_ev_after;
 extern int g_score_grid;
+extern int g_score_path;
 
 // Tensor-core scoring with the finish and the selection fused in. Returns
 // PQI_ENOTSUP when the device or driver lacks the feature, so the caller can
@@ -506,22 +585,24 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
   } else if (!w->W_hi || !w->W_lo) {
     return PQI_EINVAL;
   }
+  // CTA pairs (cta_group::2) for batches of more than one 128-candidate block,
+  // unless the single-CTA form is selected (pqi_score_set_path(2))
+  const bool pair = ntm >= 2 && g_score_path != 2;
+  const int brows = pair ? tc::BN / 2 : tc::BN;
   CUtensorMap ma, mb0, mb1;
   if (!cached_map(&ma, X, i8, shots, n, ld, tc::BM)) return PQI_ENOTSUP;
-  if (!cached_map(&mb0, i8 ? (const void*)w->W_i8 : (const void*)w->W_hi, i8, n, n, ld, tc::BN))
+  if (!cached_map(&mb0, i8 ? (const void*)w->W_i8 : (const void*)w->W_hi, i8, n, n, ld, brows))
     return PQI_ENOTSUP;
-  if (!cached_map(&mb1, i8 ? (const void*)w->W_i8 : (const void*)w->W_lo, i8, n, n, ld, tc::BN))
+  if (!cached_map(&mb1, i8 ? (const void*)w->W_i8 : (const void*)w->W_lo, i8, n, n, ld, brows))
     return PQI_ENOTSUP;
-  static bool attr_set[2] = {false, false};
-  if (!attr_set[i8]) {
-    if (i8) {
-      PQI_TRY(cudaFuncSetAttribute(tc::score_tc_kernel<true>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
-    } else {
-      PQI_TRY(cudaFuncSetAttribute(tc::score_tc_kernel<false>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
-    }
-    attr_set[i8] = true;
+  static bool attr_set[2][2] = {{false, false}, {false, false}};
+  if (!attr_set[i8][pair]) {
+    const void* k = i8 ? (pair ? (const void*)tc::score_tc_kernel<true, true>
+                               : (const void*)tc::score_tc_kernel<true, false>)
+                       : (pair ? (const void*)tc::score_tc_kernel<false, true>
+                               : (const void*)tc::score_tc_kernel<false, false>);
+    PQI_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
+    attr_set[i8][pair] = true;
   }
   PQI_TRY(cudaMemsetAsync(ctl, 0, ctl_bytes, s));
   const long long words = (long long)shots * n32;
@@ -532,16 +613,54 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     tc::expand_pm1_kernel<uint16_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (uint16_t*)X);
   }
   PQI_LAUNCHED("expand_pm1_kernel");
-  const int grid = std::min(ntn * ntm, g_score_grid > 0 ? g_score_grid : num_sms);
+  const int limit = g_score_grid > 0 ? g_score_grid : num_sms;
   if (g_score_ev_before) PQI_TRY(cudaEventRecord(g_score_ev_before, s));
-  if (i8) {
-    tc::score_tc_kernel<true><<<grid, tc::PTHREADS, tc::SMEM_BYTES, s>>>(
-        ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount, mdone,
-        key, best_energy, best_index, err);
+  if (pair) {
+    const int tiles = ntn * ((shots + 2 * tc::BM - 1) / (2 * tc::BM));
+    cudaLaunchConfig_t cfg = {};
+    cfg.blockDim = dim3(tc::PTHREADS);
+    cfg.dynamicSmemBytes = tc::SMEM_BYTES;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 2;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    // a persistent grid of exactly the pairs that can be resident at once (a
+    // pair needs two free SMs of one GPC), cached per weight kind
+    static int fit[2] = {0, 0};
+    if (!fit[i8]) {
+      cfg.gridDim = dim3(2);
+      int f = 0;
+      PQI_TRY(cudaOccupancyMaxActiveClusters(
+          &f, i8 ? (const void*)tc::score_tc_kernel<true, true> : (const void*)tc::score_tc_kernel<false, true>,
+          &cfg));
+      fit[i8] = std::max(1, f);
+    }
+    const int pairs = std::max(1, std::min({tiles, limit / 2, fit[i8]}));
+    cfg.gridDim = dim3(2 * pairs);
+    if (i8) {
+      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<true, true>, ma, mb0, mb1, n, shots,
+                                 theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
+                                 mdone, key, best_energy, best_index, err));
+    } else {
+      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<false, true>, ma, mb0, mb1, n, shots,
+                                 theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
+                                 mdone, key, best_energy, best_index, err));
+    }
   } else {
-    tc::score_tc_kernel<false><<<grid, tc::PTHREADS, tc::SMEM_BYTES, s>>>(
-        ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount, mdone,
-        key, best_energy, best_index, err);
+    const int grid = std::min(ntn * ntm, limit);
+    if (i8) {
+      tc::score_tc_kernel<true, false><<<grid, tc::PTHREADS, tc::SMEM_BYTES, s>>>(
+          ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
+          mdone, key, best_energy, best_index, err);
+    } else {
+      tc::score_tc_kernel<false, false><<<grid, tc::PTHREADS, tc::SMEM_BYTES, s>>>(
+          ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
+          mdone, key, best_energy, best_index, err);
+    }
   }
   PQI_LAUNCHED("score_tc_kernel");
   if (g_score_ev_after) PQI_TRY(cudaEventRecord(g_score_ev_after, s));

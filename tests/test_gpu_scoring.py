@@ -47,13 +47,15 @@ def test_tensor_core_scoring(n, shots, kind, oracle_mod):
         else:
             tol = 1e-5 * np.abs(W.astype(np.float64)).sum() / 2
             assert np.all(np.abs(got - exact) <= tol), np.abs(got - exact).max() / tol
-        # same answer from the CUDA-core path
-        _lib.call("pqi_score_set_path", 1)
-        try:
-            e1, be1, bi1 = dg.calculate_cut(words, shots, spin, G, L)
-        finally:
-            _lib.call("pqi_score_set_path", 0)
-        if kind == "int":
-            assert torch.equal(e1, e) and int(bi1.item()) == int(bi.item())
-        else:
-            assert np.all(np.abs(e1.cpu().numpy().astype(np.float64) - exact) <= tol)
+        # same answer from the CUDA-core path (1) and the single-CTA
+        # tensor-core path (2; the default pairs CTAs above 128 candidates)
+        for path in (1, 2):
+            _lib.call("pqi_score_set_path", path)
+            try:
+                e1, be1, bi1 = dg.calculate_cut(words, shots, spin, G, L)
+            finally:
+                _lib.call("pqi_score_set_path", 0)
+            if kind == "int":
+                assert torch.equal(e1, e) and int(bi1.item()) == int(bi.item()), path
+            else:
+                assert np.all(np.abs(e1.cpu().numpy().astype(np.float64) - exact) <= tol), path
