@@ -331,6 +331,12 @@ pqi_status pqi_batch_search_f32(const void* graphs, int num_graphs, const int* t
                                 double* best_values, unsigned long long* flips_total,
                                 int* status, void* stream);
 
+/* Tuning / cross-check knob (no reference counterpart): on (default) lets
+ * pqi_batch_search_f32 (float32 local fields) stage four row groups per thread
+ * in shared memory with cp.async for graphs of more than 4096 nodes; off keeps
+ * every row group in registers. Results are identical. */
+pqi_status pqi_batch_set_staging(int on);
+
 /*
  * pqi_batch_search with one warp per task instead of one CTA: the same search,
  * selection rule, kick stream, outputs and status, for graphs with
@@ -432,6 +438,16 @@ pqi_status pqi_tfim_jz(const float* W, int n, double* J_eff, unsigned int* degre
  * (upper-triangular) entries. */
 pqi_status pqi_tfim_jz_f32(const float* W, int n, double* J_eff, unsigned int* degrees,
                            void* workspace, size_t workspace_bytes, void* stream);
+
+/* Dense matrices of a sparse graph's stored entries (rows[e], cols[e], vals[e]),
+ * e < nnz, coordinates unique: S = the stored off-diagonal entries, W = S + S^T
+ * (both n*n float32 row-major, zeroed by the call; S nullable). Replaces the
+ * reference's CSR handling of the sparse entry points
+ * (maxcut_tfim_util.py:533-542 builds the CSR; kernels.cl:233-251 sums over it
+ * as W): the dense path then runs on W, the sampler's J / degrees on S. An
+ * out-of-range coordinate is skipped and sets *bad (device int) to 1. */
+pqi_status pqi_coo_to_dense(const int* rows, const int* cols, const float* vals, long long nnz,
+                            int n, float* S, float* W, int* bad, void* stream);
 
 /* Workspace bytes pqi_tfim_cdf needs. */
 size_t pqi_tfim_cdf_workspace_bytes(int n, int quality);

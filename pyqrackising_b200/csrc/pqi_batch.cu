@@ -59,7 +59,19 @@ struct TaskCtx {
   int n, ld;
   GT* g;  // local fields y = W x
   uint32_t* bits;
+  WT* stage;  // staged row groups (kStageGroups x 256 threads x 4 weights), or null
 };
+
+// Row groups per thread that the staged form copies with cp.async (no
+// registers held while in flight) on top of the CH groups loaded to registers.
+constexpr int kStageGroups = 4;
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(src_bytes)
+               : "memory");
+}
 
 // Node for a uniform draw u in [0, 1): from the normalised cumulative array
 // `cdf` (first entry above u) or uniformly.
@@ -105,7 +117,7 @@ __device__ __forceinline__ unsigned long long bmax_key(unsigned long long key) {
 // itself, so the next pass starts without a second barrier (a warp can be at
 // most one pass ahead of another, which writes the other slot array).
 // k < 0: no flip, only the selection. Returns the key and the exact gain.
-template <typename WT, typename GT, int CH>
+template <typename WT, typename GT, int CH, bool STG = false>
 __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k, int xk,
                                                 unsigned long long (*red_key)[8],
                                                 double (*red_g)[8], int par,
@@ -117,7 +129,48 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   int bi = -1, bx = 0;
   double bg = 0.0;
   constexpr int stride = 1024;  // 4 nodes x 256 threads
-  for (int base = 4 * threadIdx.x; base < n; base += CH * stride) {
+  // one group of four nodes v0 .. v0 + 3 with their weights of row k
+  auto group = [&](int v0, const WT* w4) {
+    if (k >= v0 && k < v0 + 4) c.bits[k >> 5] ^= 1u << (k & 31);
+    const uint32_t word = c.bits[v0 >> 5];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int v = v0 + i;
+      if (v < n) {
+        GT y = c.g[fpos(v)];
+        if (k >= 0) {
+          y += coef * (GT)w4[i];
+          c.g[fpos(v)] = y;
+        }
+        const int xv = (word >> (v & 31)) & 1;
+        const double g = xv ? (double)y : -(double)y;
+        const float gv = (float)g;
+        if (gv > bv) {  // v ascends within a thread: strict '>' keeps the lowest node
+          bv = gv;
+          bi = v;
+          bg = g;
+          bx = xv;
+        }
+      }
+    }
+  };
+  constexpr int PER = STG ? CH + kStageGroups : CH;  // groups per pass
+  for (int base = 4 * threadIdx.x; base < n; base += PER * stride) {
+    if constexpr (STG) {
+      // the pass's last kStageGroups groups go to shared memory first, so the
+      // whole pass is in flight while the register groups are waited on; each
+      // thread reads back only the slots it copied itself
+      if (k >= 0) {
+#pragma unroll
+        for (int j = 0; j < kStageGroups; ++j) {
+          const int v = base + (CH + j) * stride;
+          if (v < n)
+            cp_async16(c.stage + (size_t)(j * 256 + threadIdx.x) * 4, row + v,
+                       (n - v) >= 4 ? 16 : (n - v) * (int)sizeof(WT));
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      }
+    }
     WT w[4 * CH];
     if (k >= 0) {
 #pragma unroll
@@ -140,28 +193,21 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
 #pragma unroll
     for (int j = 0; j < CH; ++j) {
       const int v0 = base + j * stride;
-      if (v0 < n) {
-        if (k >= v0 && k < v0 + 4) c.bits[k >> 5] ^= 1u << (k & 31);
-        const uint32_t word = c.bits[v0 >> 5];
+      if (v0 < n) group(v0, w + 4 * j);
+    }
+    if constexpr (STG) {
+      if (k >= 0) asm volatile("cp.async.wait_group 0;" ::: "memory");
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int v = v0 + i;
-          if (v < n) {
-            GT y = c.g[fpos(v)];
-            if (k >= 0) {
-              y += coef * (GT)w[4 * j + i];
-              c.g[fpos(v)] = y;
-            }
-            const int xv = (word >> (v & 31)) & 1;
-            const double g = xv ? (double)y : -(double)y;
-            const float gv = (float)g;
-            if (gv > bv) {  // v ascends within a thread: strict '>' keeps the lowest node
-              bv = gv;
-              bi = v;
-              bg = g;
-              bx = xv;
-            }
+      for (int j = 0; j < kStageGroups; ++j) {
+        const int v0 = base + (CH + j) * stride;
+        if (v0 < n) {
+          WT w4[4] = {(WT)0, (WT)0, (WT)0, (WT)0};
+          if (k >= 0) {
+            const float4 t =
+                *reinterpret_cast<const float4*>(c.stage + (size_t)(j * 256 + threadIdx.x) * 4);
+            w4[0] = t.x; w4[1] = t.y; w4[2] = t.z; w4[3] = t.w;
           }
+          group(v0, w4);
         }
       }
     }
@@ -184,7 +230,10 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
 // F32: float graphs keep float32 local fields (half the shared memory and
 // fewer registers, so more resident tasks per SM); gains, the selection rule
 // and the float64 running value are unchanged in form.
-template <typename WT, int CH, bool F32>
+// STG (float32 fields only): each flip pass also stages kStageGroups row
+// groups per thread through cp.async, so a pass of SK n = 8192 has its whole
+// 32 KB row in flight at once instead of in two register chunks.
+template <typename WT, int CH, bool F32, bool STG = false>
 __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
     const BatchGraph* __restrict__ graphs, const int* __restrict__ task_graph,
     const uint32_t* __restrict__ init_states, int words_pitch, int tasks, int spin, int rounds,
@@ -209,6 +258,10 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
     c.g = reinterpret_cast<GT*>(smem + (((size_t)n32 * 4 + 15) & ~size_t(15)));
     uint32_t* kicked = reinterpret_cast<uint32_t*>(
         smem + (((size_t)n32 * 4 + 15) & ~size_t(15)) + (size_t)((n + 1023) / 1024 * 1024) * sizeof(GT));
+    static_assert(!STG || (F32 && sizeof(WT) == 4), "staged groups: float rows, float32 fields");
+    c.stage = STG ? reinterpret_cast<WT*>(reinterpret_cast<unsigned char*>(kicked) +
+                                          (((size_t)n32 * 4 + 15) & ~size_t(15)))
+                  : nullptr;
     uint32_t* best_bits = best_states + (size_t)task * words_pitch;
     for (int w = threadIdx.x; w < n32; w += blockDim.x) c.bits[w] = init_states[(size_t)task * words_pitch + w];
     __syncthreads();
@@ -292,7 +345,7 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
     unsigned long long key;
     double gk;
     int par = 0;
-    flip_and_select<WT, GT, CH>(c, -1, 0, red_key, red_g, par, &key, &gk);
+    flip_and_select<WT, GT, CH, STG>(c, -1, 0, red_key, red_g, par, &key, &gk);
     par ^= 1;
     for (int r = 0; r <= rounds; ++r) {
       // steepest ascent: flip the best node while its gain is positive
@@ -304,7 +357,7 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
         }
         const int k = (int)(0x3FFFFFFFu - (((uint32_t)key) >> 1));
         val += scale * gk;  // exact gain of k before the flip
-        flip_and_select<WT, GT, CH>(c, k, (int)(key & 1ull), red_key, red_g, par, &key, &gk);
+        flip_and_select<WT, GT, CH, STG>(c, k, (int)(key & 1ull), red_key, red_g, par, &key, &gk);
         par ^= 1;
         ++nflips;
       }
@@ -331,7 +384,7 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
         __syncthreads();  // everyone has read bit, field and kicked set before they change
         if (threadIdx.x == 0) kicked[pick >> 5] |= 1u << (pick & 31);
         val += scale * gp;
-        flip_and_select<WT, GT, CH>(c, pick, xp, red_key, red_g, par, &key, &gk);
+        flip_and_select<WT, GT, CH, STG>(c, pick, xp, red_key, red_g, par, &key, &gk);
         par ^= 1;
         ++nflips;
       }
@@ -559,6 +612,8 @@ size_t pqi_batch_graph_desc_bytes(void) { return sizeof(BatchGraph); }
 
 }  // extern "C"
 
+static int g_batch_no_stage = 0;
+
 static pqi_status batch_search_impl(const void* graphs, int num_graphs, const int* task_graph,
                                     const uint32_t* init_states, int words_pitch, int tasks,
                                     int max_n, int kind, int is_spin_glass, int rounds, int kick,
@@ -575,8 +630,13 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   const size_t smem = (((size_t)((max_n + 31) >> 5) * 4 + 15) & ~size_t(15)) +
                       (size_t)((max_n + 1023) / 1024 * 1024) *
                           (i8 ? sizeof(int) : (f32 ? sizeof(float) : sizeof(double))) +
-                      (size_t)((max_n + 31) >> 5) * 4;  // kicked set of the current round
-  PQI_CHECK_ARG(smem <= 200 * 1024);
+                      (((size_t)((max_n + 31) >> 5) * 4 + 15) & ~size_t(15));  // kicked set of the round
+  const int groups = (max_n + 1023) / 1024;  // groups of four per thread
+  // float32 fields beyond four groups: four more groups per pass staged in
+  // shared memory (16 KB), all of SK n = 8192's row in flight per flip
+  const bool staged = f32 && !i8 && groups > 4 && !g_batch_no_stage;
+  const size_t smem_all = smem + (staged ? (size_t)kStageGroups * 256 * 4 * sizeof(float) : 0);
+  PQI_CHECK_ARG(smem_all <= 200 * 1024);
   static int num_sms = 0;
   if (!num_sms) {
     int dev = 0;
@@ -590,38 +650,39 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   // (the whole row for n <= 4 * 256 * CH). CH = 4 keeps three CTAs per SM
   // within the register file (8 groups spill at that occupancy and run slower
   // on SK n = 8192 than two chunks of 4).
-#define PQI_BATCH_LAUNCH(WT_, CH_, F_)                                                          \
+#define PQI_BATCH_LAUNCH(WT_, CH_, F_, S_)                                                      \
   do {                                                                                         \
-    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_>,                               \
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
-    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_>,                               \
+    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_, S_>,                        \
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_all)); \
+    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_, S_>,                        \
                                  cudaFuncAttributePreferredSharedMemoryCarveout, 100));        \
-    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_search_kernel<WT_, CH_, F_>, \
-                                                          256, smem));                         \
+    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                     \
+        &per_sm, batch_search_kernel<WT_, CH_, F_, S_>, 256, smem_all));                       \
     const int grid = std::max(1, std::min(tasks, num_sms * std::max(1, per_sm)));             \
-    batch_search_kernel<WT_, CH_, F_><<<grid, 256, smem, s>>>(                                     \
+    batch_search_kernel<WT_, CH_, F_, S_><<<grid, 256, smem_all, s>>>(                         \
         gd, task_graph, init_states, words_pitch, tasks, is_spin_glass, rounds, kick,          \
         flip_budget, seed, kick_cdf, cdf_offset, best_states, best_values, flips_total,        \
         status);                                                                               \
   } while (0)
-  const int groups = (max_n + 1023) / 1024;  // groups of four per thread
   if (i8) {
     if (groups <= 2) {
-      PQI_BATCH_LAUNCH(int8_t, 2, false);
+      PQI_BATCH_LAUNCH(int8_t, 2, false, false);
     } else {
-      PQI_BATCH_LAUNCH(int8_t, 4, false);
+      PQI_BATCH_LAUNCH(int8_t, 4, false, false);
     }
   } else if (f32) {
     if (groups <= 2) {
-      PQI_BATCH_LAUNCH(float, 2, true);
+      PQI_BATCH_LAUNCH(float, 2, true, false);
+    } else if (staged) {
+      PQI_BATCH_LAUNCH(float, 4, true, true);
     } else {
-      PQI_BATCH_LAUNCH(float, 4, true);
+      PQI_BATCH_LAUNCH(float, 4, true, false);
     }
   } else {
     if (groups <= 2) {
-      PQI_BATCH_LAUNCH(float, 2, false);
+      PQI_BATCH_LAUNCH(float, 2, false, false);
     } else {
-      PQI_BATCH_LAUNCH(float, 4, false);
+      PQI_BATCH_LAUNCH(float, 4, false, false);
     }
   }
 #undef PQI_BATCH_LAUNCH
@@ -630,6 +691,11 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
 }
 
 extern "C" {
+
+pqi_status pqi_batch_set_staging(int on) {
+  g_batch_no_stage = on ? 0 : 1;
+  return PQI_OK;
+}
 
 pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_graph,
                             const uint32_t* init_states, int words_pitch, int tasks, int max_n,

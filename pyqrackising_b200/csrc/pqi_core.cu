@@ -248,26 +248,70 @@ __global__ void select_finish_kernel(const unsigned long long* key, SelGeom geo,
 }
 
 // ---------------------------------------------------------------------------
-// Double flips: one block per row k, threads over l > k.
+// Double flips: each block takes rows k and n - 2 - k together (n pair values
+// per block, whatever k), threads over l > k. The pair value is read from the
+// maintained gains: flipping k and l gains g_k + g_l - 2 x_k x_l W_kl.
+//
+// The selection key of pair index i (sel_key) needs i mod G and i / G, and the
+// slot's tie rank. TAB: both are carried incrementally along a thread's l
+// sequence (i advances by the block size each step), and a table in shared
+// memory maps the slot t = i mod G to (group * L + rank) * J (or "never wins"),
+// so the inner loop has no division. Pair indices are below G * J < 2^32.
 
-template <typename WT>
-__global__ void double_kernel(const WT* __restrict__ Wp, int ld, int n,
+constexpr int kDoubleTab = 2048;  // slots the table holds; a larger G takes the direct key
+
+template <typename WT, bool TAB>
+__global__ void __launch_bounds__(256) double_kernel(const WT* __restrict__ Wp, int ld, int n,
                               const uint32_t* __restrict__ theta, const double* __restrict__ g64,
                               int spin, SelGeom geo, unsigned long long* key) {
   __shared__ uint64_t scratch[32];
+  __shared__ uint32_t tab[TAB ? kDoubleTab : 1];
+  if constexpr (TAB) {
+    for (uint32_t t = threadIdx.x; t < geo.G; t += blockDim.x) {
+      const uint32_t grp = t / geo.L;
+      const uint32_t r = geo.rank[t - grp * geo.L];
+      tab[t] = (r == 0xFFu) ? 0xFFFFFFFFu : (grp * geo.L + r) * geo.J;
+    }
+  }
+  __syncthreads();
+  const uint32_t step_t = blockDim.x % geo.G, step_j = blockDim.x / geo.G;
   uint64_t best = 0;
-  for (int k = blockIdx.x; k < n - 1; k += gridDim.x) {
-    const double gk = g64[k];
-    const int xk = get_bit32(theta, k);
-    const long long base = pair_base(k, n) - (k + 1);
-    const WT* row = Wp + (size_t)k * ld;
-    for (int l = k + 1 + threadIdx.x; l < n; l += blockDim.x) {
-      const double w = (double)row[l];
-      const double d = gk + __ldg(g64 + l) - ((get_bit32(theta, l) == xk) ? 2.0 * w : -2.0 * w);
-      float v = (float)d;
-      if (spin) v *= 2.0f;
-      const uint64_t kk = sel_key(v, (uint64_t)(base + l), geo);
-      best = kk > best ? kk : best;
+  const int half = n >> 1;  // row pairs (p, n - 2 - p), p < half; one row when they meet
+  for (int p = blockIdx.x; p < half; p += gridDim.x) {
+    for (int side = 0; side < 2; ++side) {
+      const int k = side ? n - 2 - p : p;
+      if (side && k == p) continue;
+      const double gk = g64[k];
+      const int xk = get_bit32(theta, k);
+      const uint32_t base = (uint32_t)(pair_base(k, n) - (k + 1));  // pair (k, l) = base + l
+      const WT* row = Wp + (size_t)k * ld;
+      int l = k + 1 + threadIdx.x;
+      uint32_t i = base + (uint32_t)l;
+      uint32_t t = i % geo.G, j = i / geo.G;
+#pragma unroll 4
+      for (; l < n; l += blockDim.x) {
+        const double w = (double)row[l];
+        const double d = gk + __ldg(g64 + l) - ((get_bit32(theta, l) == xk) ? 2.0 * w : -2.0 * w);
+        float v = (float)d;
+        if (spin) v *= 2.0f;
+        uint64_t kk;
+        if constexpr (TAB) {
+          const uint32_t pr = tab[t];
+          kk = (pr == 0xFFFFFFFFu || v != v)
+                   ? 0ull
+                   : (((uint64_t)ord_f32(v) << 32) | (uint64_t)(0xFFFFFFFFu - (pr + j)));
+        } else {
+          kk = sel_key(v, (uint64_t)i, geo);
+        }
+        best = kk > best ? kk : best;
+        i += blockDim.x;
+        t += step_t;
+        j += step_j;
+        if (t >= geo.G) {
+          t -= geo.G;
+          ++j;
+        }
+      }
     }
   }
   best = block_max_u64(best, scratch);
@@ -593,13 +637,22 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     gains64 = g;
   }
   PQI_TRY(cudaMemsetAsync(key, 0, sizeof(unsigned long long), s));
-  const int grid = std::min(n - 1, 148 * 16);
+  const int grid = std::max(1, std::min(n >> 1, 148 * 8));
+  const bool tab = geo.G <= (uint32_t)kDoubleTab;
   if (w->kind == PQI_W_I8) {
-    double_kernel<int8_t><<<grid, 256, 0, s>>>(w->W_i8, w->ld, n, theta, gains64,
-                                               is_spin_glass, geo, key);
+    if (tab)
+      double_kernel<int8_t, true><<<grid, 256, 0, s>>>(w->W_i8, w->ld, n, theta, gains64,
+                                                       is_spin_glass, geo, key);
+    else
+      double_kernel<int8_t, false><<<grid, 256, 0, s>>>(w->W_i8, w->ld, n, theta, gains64,
+                                                        is_spin_glass, geo, key);
   } else {
-    double_kernel<float><<<grid, 256, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64,
-                                              is_spin_glass, geo, key);
+    if (tab)
+      double_kernel<float, true><<<grid, 256, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64,
+                                                      is_spin_glass, geo, key);
+    else
+      double_kernel<float, false><<<grid, 256, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64,
+                                                       is_spin_glass, geo, key);
   }
   PQI_LAUNCHED("double_kernel");
   select_finish_kernel<<<1, 1, 0, s>>>(key, geo, best_energy, best_index);

@@ -26,11 +26,18 @@ from . import device as D
 from .util import HEURISTIC_THRESHOLD, as_matrix, get_cut
 
 
+def _as_device_f32(M, dev):
+    """A host array or a torch tensor as a contiguous float32 tensor on `dev`."""
+    if isinstance(M, torch.Tensor):
+        return M.detach().to(device=dev, dtype=torch.float32).contiguous()
+    return torch.from_numpy(np.ascontiguousarray(M, dtype=np.float32)).to(dev)
+
+
 def exact_search(G_m, is_spin_glass: bool, device=None):
     """(bool[n], best value) of exact_maxcut / exact_spin_glass (maxcut_tfim.py:288-339)."""
     dev = torch.device(device) if device is not None else D.default_device()
     n = len(G_m)
-    W = torch.from_numpy(np.ascontiguousarray(G_m, dtype=np.float32)).to(dev)
+    W = _as_device_f32(G_m, dev)
     val = torch.empty(1, dtype=torch.float64, device=dev)
     mask = torch.empty(1, dtype=torch.int32, device=dev)
     ws = torch.empty(4096, dtype=torch.uint8, device=dev)
@@ -66,11 +73,13 @@ def maxcut_tfim(
 
 
 def _maxcut_tfim(nodes, G_m, quality, shots, is_spin_glass, anneal_t, anneal_h, repulsion_base,
-                 threshold=HEURISTIC_THRESHOLD, jz_matrix=None):
-    """maxcut_tfim on a dense symmetric matrix. `threshold` is the size below
-    which the exhaustive search runs; `jz_matrix` (default G_m) is the matrix
-    whose rows give the sampler's J_eff and degrees (the sparse entry point
-    passes the upper triangle, as the reference's sparse path reads it)."""
+                 threshold=HEURISTIC_THRESHOLD, jz_matrix=None, dg=None):
+    """maxcut_tfim on a dense symmetric matrix (host array or device tensor).
+    `threshold` is the size below which the exhaustive search runs;
+    `jz_matrix` (default G_m) is the matrix whose rows give the sampler's J_eff
+    and degrees (the sparse entry point passes the upper triangle, as the
+    reference's sparse path reads it); `dg` is G_m already prepared on the
+    device (the solver shares its own)."""
     n_qubits = len(G_m)
 
     if n_qubits < threshold:
@@ -91,10 +100,11 @@ def _maxcut_tfim(nodes, G_m, quality, shots, is_spin_glass, anneal_t, anneal_h, 
     if repulsion_base is None:
         repulsion_base = 5.0
 
-    dg = D.DeviceGraph(G_m)
+    if dg is None:
+        dg = D.DeviceGraph(G_m)
     jz = None
     if jz_matrix is not None:
-        jz = torch.from_numpy(np.ascontiguousarray(jz_matrix, dtype=np.float32)).to(dg.device)
+        jz = _as_device_f32(jz_matrix, dg.device)
     best_solution, best_value = sample_and_score(
         dg, int(quality), int(shots), bool(is_spin_glass), float(anneal_t), float(anneal_h), float(repulsion_base),
         jz_W=jz,

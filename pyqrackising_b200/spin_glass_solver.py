@@ -199,19 +199,19 @@ def _spin_glass_solver(nodes, G_m, quality, shots, best_guess, is_maxcut_gpu, is
 
     theta = parse_best_guess(best_guess, n_qubits)
     cut_value = None
+    dg = D.DeviceGraph(G_m)  # prepared once, shared by the seed sampler and the search
     if theta is None:
         bitstring, cut_value, _ = _maxcut_tfim(
             list(range(n_qubits)), G_m, quality, shots, is_spin_glass, anneal_t, anneal_h, repulsion_base,
-            threshold=threshold, jz_matrix=jz_matrix,
+            threshold=threshold, jz_matrix=jz_matrix, dg=dg,
         )
         if bp_scale is not None and n_qubits >= threshold:
             # keep whichever of the BP partition and the sample scores higher
             # (spin_glass_solver.py:493-523)
             bp_theta = bp_warm_start_dense(G_m, n_qubits, bp_scale, bp_damping)
             sample_theta = np.array([b == "1" for b in bitstring], dtype=np.bool_)
-            dgb = D.DeviceGraph(G_m)
-            cb, eb = dgb.rescore(dgb.pack(bp_theta))
-            cs, es = dgb.rescore(dgb.pack(sample_theta))
+            cb, eb = dg.rescore(dg.pack(bp_theta))
+            cs, es = dg.rescore(dg.pack(sample_theta))
             bp_energy = float(eb.item()) if is_spin_glass else float(cb.item())
             sample_energy = float(es.item()) if is_spin_glass else float(cs.item())
             if bp_energy > sample_energy:
@@ -219,7 +219,6 @@ def _spin_glass_solver(nodes, G_m, quality, shots, best_guess, is_maxcut_gpu, is
                 cut_value = bp_energy if not is_spin_glass else None
         theta = np.array([b == "1" for b in bitstring], dtype=np.bool_)
 
-    dg = D.DeviceGraph(G_m)
     words = dg.pack(theta)
     cut0, en0 = dg.rescore(words)
     if is_spin_glass:

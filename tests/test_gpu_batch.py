@@ -243,3 +243,35 @@ def test_float32_fields_form(kind, oracle_mod):
         Wd = W.astype(np.float64).copy()
         np.fill_diagonal(Wd, 0.0)
         assert np.all(x * (Wd @ x) <= 1e-5 * np.abs(Wd).sum(axis=1).max())
+
+
+def test_float32_fields_staged_rows_match_register_rows():
+    """Graphs above 4096 nodes (one with a ragged last group): the float32
+    form with four row groups per thread staged through cp.async returns the
+    same states, values and flip counts as with every group in registers, and
+    its states are local optima of the float64 objective."""
+    from pyqrackising_b200 import _lib
+    from pyqrackising_b200 import workloads as wl
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    Ws = [wl.gnp_weighted(4099, 0.2, seed=21, dist="normal"), wl.gnp_weighted(9001, 0.05, seed=22, dist="normal")]
+    bs = BatchedSearch([DeviceGraph(W) for W in Ws])
+    task_graph = [0, 1, 1, 0, 1]
+    words = bs.random_states(task_graph, seed=6)
+    try:
+        _lib.call("pqi_batch_set_staging", 0)
+        va, ba, fa, sa = bs.run(task_graph, words, True, rounds=1, kick=8, seed=2, fields="f32")
+        _lib.call("pqi_batch_set_staging", 1)
+        vb, bb, fb, sb = bs.run(task_graph, words, True, rounds=1, kick=8, seed=2, fields="f32")
+    finally:
+        _lib.call("pqi_batch_set_staging", 1)
+    assert int(sa.item()) == 0 and int(sb.item()) == 0
+    assert torch.equal(ba, bb) and torch.equal(va, vb) and int(fa.item()) == int(fb.item())
+    for t, g in enumerate(task_graph):
+        bits = bs.unpack(bb, task_graph)[t]
+        W = Ws[g].astype(np.float64)
+        np.fill_diagonal(W, 0.0)
+        x = np.where(bits, 1.0, -1.0)
+        assert float(vb[t]) == pytest.approx(-0.5 * x @ W @ x, rel=1e-5)
+        assert np.all(x * (W @ x) <= 1e-5 * np.abs(W).sum(axis=1).max())

@@ -229,3 +229,31 @@ def test_errors_are_reported_and_context_survives():
     cut, _ = dg.rescore(words)
     assert float(cut.item()) == 0.0
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("mpe", [148, 4096])
+def test_double_flips_wide_geometry(mpe, oracle_mod):
+    """n = 2200 with integer weights (exact pair values): the pair scan's
+    selection against the reference's per-work-item fold over all pairs in
+    k-major order, for a table-held geometry (G = 160) and one above the table
+    (G = 2208)."""
+    O = oracle_mod
+    n = 2200
+    rng = np.random.default_rng(11)
+    U = np.triu(rng.choice(np.array([-2.0, -1.0, 0.0, 1.0, 3.0], dtype=np.float32), size=(n, n)), 1)
+    W = U + U.T
+    th = rng.random(n) < 0.5
+    dg = _graph(W)
+    words = dg.pack(th)
+    _, g64 = dg.gains(words)
+    x = np.where(th, 1.0, -1.0)
+    g = x * (W.astype(np.float64) @ x)
+    assert np.array_equal(g64.cpu().numpy(), g)
+    k, l = np.triu_indices(n, 1)
+    vals = g[k] + g[l] - np.where(th[k] == th[l], 2.0, -2.0) * W[k, l]
+    G, L = O.flip_geometry(n, mpe)
+    assert (G > 2048) == (mpe == 4096)
+    for spin in (0, 1):
+        ke, ki = O.select((vals * (2.0 if spin else 1.0)).astype(np.float32), G, L)
+        be, bi = dg.double_bit_flips(words, g64, spin, G, L)
+        assert (float(be.item()), int(bi.item())) == (float(ke), int(ki))

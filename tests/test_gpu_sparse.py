@@ -85,3 +85,48 @@ def test_sampling_path_returns_a_rescored_cut(oracle_mod):
     sol = np.array([c == "1" for c in bits])
     assert val == pytest.approx(O.compute_cut(sol, U + U.T), rel=1e-6, abs=1e-6)
     assert len(l) + len(r) == U.shape[0]
+
+
+def test_device_expansion_equals_the_host_expansion():
+    """pqi_coo_to_dense builds W and S bit for bit as the host does, for graph
+    and matrix inputs and both triangles stored; repeated coordinates take the
+    host path; an out-of-range coordinate is reported, not written."""
+    import ctypes
+
+    import networkx as nx
+    import torch
+    from scipy.sparse import coo_matrix, csr_matrix
+
+    from pyqrackising_b200 import _lib
+    from pyqrackising_b200 import device as D
+    from pyqrackising_b200.sparse import sparse_to_dense, sparse_to_device
+
+    z = np.load(GOLD)
+    rng = np.random.default_rng(3)
+    cases = []
+    for i in range(int(z["count"])):
+        U = z[f"U{i}"]
+        cases += [csr_matrix(U), csr_matrix(U + U.T)]
+        g = nx.Graph()
+        g.add_nodes_from(range(U.shape[0]))
+        for a, b in zip(*np.nonzero(U)):
+            g.add_edge(int(b), int(a), weight=float(U[a, b]))
+        cases.append(g)
+    n = 300
+    r, c = rng.integers(0, n, 4000), rng.integers(0, n, 4000)
+    cases.append(csr_matrix((rng.standard_normal(4000).astype(np.float32), (r, c)), shape=(n, n)))
+    cases.append(coo_matrix((rng.standard_normal(4000).astype(np.float32), (r, c)), shape=(n, n)))
+    for G in cases:
+        _, W, S = sparse_to_dense(G)
+        _, Wd, Sd = sparse_to_device(G)
+        assert np.array_equal(Wd.cpu().numpy().view(np.uint32), W.view(np.uint32))
+        assert np.array_equal(Sd.cpu().numpy().view(np.uint32), S.view(np.uint32))
+    rows = torch.tensor([0, 5, 1], dtype=torch.int32, device="cuda")
+    cols = torch.tensor([1, 0, 2], dtype=torch.int32, device="cuda")
+    vals = torch.tensor([1.0, 2.0, 3.0], dtype=torch.float32, device="cuda")
+    W = torch.empty((3, 3), dtype=torch.float32, device="cuda")
+    bad = torch.empty(1, dtype=torch.int32, device="cuda")
+    _lib.call("pqi_coo_to_dense", D._ptr(rows), D._ptr(cols), D._ptr(vals), ctypes.c_longlong(3), 3,
+              None, D._ptr(W), D._ptr(bad), D.stream_ptr())
+    assert int(bad.item()) == 1
+    assert W.cpu().numpy().tolist() == [[0.0, 1.0, 0.0], [1.0, 0.0, 3.0], [0.0, 3.0, 0.0]]

@@ -51,3 +51,34 @@ def test_dense_objectives_equal_reference_sparse_objectives(oracle_mod):
         for s, c, e in zip(z[f"states{i}"], z[f"cut{i}"], z[f"energy{i}"]):
             assert O.compute_cut(s, W) == pytest.approx(c, abs=tol)
             assert O.compute_energy(s, W) == pytest.approx(e, abs=tol)
+
+
+def test_coordinate_list_rebuilds_the_host_expansion():
+    """The coordinate list that crosses to the device holds exactly the host
+    expansion's stored entries (graph and matrix inputs; repeats flagged)."""
+    import networkx as nx
+    from scipy.sparse import coo_matrix, csr_matrix
+
+    from pyqrackising_b200.sparse import sparse_coordinates, sparse_to_dense
+
+    z, count = _cases()
+    cases = []
+    for i in range(count):
+        U = z[f"U{i}"]
+        cases.append(csr_matrix(U))
+        cases.append(csr_matrix(U + U.T))  # both halves stored
+        g = nx.Graph()
+        g.add_nodes_from(range(U.shape[0]))
+        for a, b in zip(*np.nonzero(U)):
+            g.add_edge(int(b), int(a), weight=float(U[a, b]))  # reversed endpoints
+        cases.append(g)
+    for G in cases:
+        nodes, n, rows, cols, vals, unique = sparse_coordinates(G)
+        assert unique
+        _, W, S = sparse_to_dense(G)
+        S2 = np.zeros((n, n), dtype=np.float32)
+        S2[rows, cols] = vals
+        assert np.array_equal(S2, S) and np.array_equal(S2 + S2.T, W)
+    dup = coo_matrix((np.array([1.0, 2.0, 3.0], dtype=np.float32), (np.array([0, 0, 1]), np.array([1, 1, 2]))),
+                     shape=(3, 3))
+    assert not sparse_coordinates(dup)[5]
