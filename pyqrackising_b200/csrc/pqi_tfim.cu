@@ -278,6 +278,9 @@ __device__ __forceinline__ int sample_mag(const double* cum, int len, double p) 
   return m;
 }
 
+constexpr int kWtsPitch = 33;  // doubles per row of a warp's weight table (32 lanes + 1)
+constexpr int kRowBatch = 16;  // row steps of 32 weights in flight per repulsion update
+
 __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
                                    const double* __restrict__ cum, int ncum, double base,
                                    int repel, uint64_t seed, uint64_t round, int shots,
@@ -289,9 +292,10 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
   const int wpb = blockDim.x >> 5;
   const int C = (n + 31) >> 5;
   const int n32 = C;  // words per packed row == nodes per lane chunk, both ceil(n/32)
-  double* wts = use_smem ? reinterpret_cast<double*>(smem) + (size_t)wib * (C * 32)
-                         : wglob + (size_t)(blockIdx.x * wpb + wib) * (C * 32);
+  double* wts = use_smem ? reinterpret_cast<double*>(smem) + (size_t)wib * (C * kWtsPitch)
+                         : wglob + (size_t)(blockIdx.x * wpb + wib) * (C * kWtsPitch);
   const double lnb = log(base);
+  const double rep1 = exp(-lnb);  // repulsion factor of a unit weight
   for (int s = blockIdx.x * wpb + wib; s < shots; s += gridDim.x * wpb) {
     const int m = sample_mag(cum, ncum, uniform(seed, round, (uint64_t)s, 0));
     const int node0 = s % n;
@@ -300,8 +304,11 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
       for (int w = lane; w < n32; w += 32) out[w] = (w == (node0 >> 5)) ? (1u << (node0 & 31)) : 0u;
       continue;
     }
+    // lane l owns nodes v0 .. v0 + C - 1 (the bisection's order); node v0 + i
+    // is stored at wts[i * 33 + l]: the owners' sweeps (fixed i, 32 lanes) and
+    // the node-order sweeps (32 consecutive nodes) both spread over the banks
     const int v0 = lane * C;
-    for (int i = 0; i < C; ++i) wts[v0 + i] = (v0 + i < n) ? 1.0 : 0.0;
+    for (int i = 0; i < C; ++i) wts[i * kWtsPitch + lane] = (v0 + i < n) ? 1.0 : 0.0;
     __syncwarp();
     // picks after the first node: m - 1 for m >= 2, one for m == 0 (the loop of
     // local_repulsion_choice runs max(0, m - 2) times, then one last pick)
@@ -311,7 +318,7 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
       if (j > 0) {
         // bit_pick (util:711-724): p = sum(weights) * u, first i with p < running sum
         double loc = 0.0;
-        for (int i = 0; i < C; ++i) loc += wts[v0 + i];
+        for (int i = 0; i < C; ++i) loc += wts[i * kWtsPitch + lane];
         double incl = loc;
         for (int o = 1; o < 32; o <<= 1) {
           const double y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
@@ -327,7 +334,7 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
             double run = incl - loc;
             picked = v0;
             for (int i = 0; i < C; ++i) {
-              run += wts[v0 + i];
+              run += wts[i * kWtsPitch + lane];
               if (p < run) {
                 picked = v0 + i;
                 break;
@@ -340,15 +347,30 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
       }
       // update_repulsion_choice (maxcut_tfim.py:37-45) for all but the last pick
       __syncwarp();
-      if (lane == (node / C)) wts[node] = 0.0;
+      if (lane == (node / C)) wts[(node - lane * C) * kWtsPitch + lane] = 0.0;
       __syncwarp();
       if (j < picks && repel) {
+        // the row in node order, 32 consecutive weights per step (coalesced),
+        // kRowBatch steps loaded before any is applied (the weight table may
+        // be global memory, so loads would otherwise wait behind the stores);
+        // each lane scales the weight of its node v wherever v's owner keeps it
         const float* row = W + (size_t)node * n;
-        for (int i = 0; i < C; ++i) {
-          const int v = v0 + i;
-          if (v < n) {
-            const float wv = row[v];
-            if (wv != 0.0f) wts[v] *= (wv == 1.0f) ? exp(-lnb) : exp(-lnb * (double)wv);
+        int q = lane / C, r = lane - q * C;  // v = lane + 32 w = q C + r
+        const int dq = 32 / C, dr = 32 - dq * C;
+        for (int vb = lane; vb < n; vb += 32 * kRowBatch) {
+          float wv[kRowBatch];
+#pragma unroll
+          for (int u = 0; u < kRowBatch; ++u) wv[u] = (vb + 32 * u < n) ? __ldg(row + vb + 32 * u) : 0.0f;
+#pragma unroll
+          for (int u = 0; u < kRowBatch; ++u) {
+            if (wv[u] != 0.0f)
+              wts[r * kWtsPitch + q] *= (wv[u] == 1.0f) ? rep1 : exp(-lnb * (double)wv[u]);
+            q += dq;
+            r += dr;
+            if (r >= C) {
+              r -= C;
+              ++q;
+            }
           }
         }
       }
@@ -357,7 +379,7 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
     // selection mask: weights == 0 (picked, or underflowed to zero)
     for (int w = 0; w < n32; ++w) {
       const int v = w * 32 + lane;
-      const bool sel = v < n && wts[v] == 0.0;
+      const bool sel = v < n && wts[(v % C) * kWtsPitch + v / C] == 0.0;
       const unsigned bits = __ballot_sync(0xFFFFFFFFu, sel);
       if (lane == 0) out[w] = bits;
     }
@@ -444,7 +466,7 @@ pqi_status pqi_tfim_cdf(const double* J_eff, const unsigned int* degrees, int n,
 
 size_t pqi_tfim_sample_workspace_bytes(int n) {
   const int C = (n + 31) / 32;
-  return (size_t)148 * 16 * 32 * C * sizeof(double) + 4096;
+  return (size_t)148 * 16 * kWtsPitch * C * sizeof(double) + 4096;
 }
 
 pqi_status pqi_tfim_sample(const float* W, int n, const double* cum, double repulsion_base,
@@ -453,7 +475,7 @@ pqi_status pqi_tfim_sample(const float* W, int n, const double* cum, double repu
   PQI_CHECK_ARG(W && cum && theta_out && n >= 3 && shots > 0);
   cudaStream_t s = as_stream(stream);
   const int C = (n + 31) / 32;
-  const size_t per_warp = (size_t)C * 32 * sizeof(double);
+  const size_t per_warp = (size_t)C * kWtsPitch * sizeof(double);
   const int repel = fabs(1.0 - repulsion_base) <= kEps ? 0 : 1;
   int wpb = 4;
   size_t smem = per_warp * wpb;
@@ -476,7 +498,7 @@ pqi_status pqi_tfim_sample(const float* W, int n, const double* cum, double repu
     const long long warps = std::min<long long>((long long)(avail / per_warp), 148 * 16);
     PQI_CHECK_ARG(warps >= wpb);
     grid = (int)std::min<long long>(warps / wpb, ((long long)shots + wpb - 1) / wpb);
-    wglob = ws.take<double>((size_t)grid * wpb * C * 32);
+    wglob = ws.take<double>((size_t)grid * wpb * C * kWtsPitch);
     PQI_CHECK_ARG(wglob);
   }
   tfim_sample_kernel<<<grid, 32 * wpb, smem, s>>>(W, n, cum, n - 1, repulsion_base, repel, seed,
