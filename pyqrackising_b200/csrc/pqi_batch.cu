@@ -18,6 +18,7 @@
 // for int8 weights and float64 otherwise. Every loop is bounded (flip budget
 // per ascent).
 #include <algorithm>
+#include <climits>
 #include <type_traits>
 
 #include "pqi_common.cuh"
@@ -128,6 +129,12 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   float bv = -INFINITY;
   int bi = -1, bx = 0;
   double bg = 0.0;
+  // The selection compares gains as float32, lowest node on ties. Per field
+  // type the comparison uses as few conversions as give the same result:
+  // float fields compare in float (no conversion); int fields compare as int
+  // (exact in float below 2^24, more than 127 x the largest n); double fields
+  // round each gain to float once.
+  int bint = INT_MIN;
   constexpr int stride = 1024;  // 4 nodes x 256 threads
   // one group of four nodes v0 .. v0 + 3 with their weights of row k
   auto group = [&](int v0, const WT* w4) {
@@ -143,13 +150,30 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
           c.g[fpos(v)] = y;
         }
         const int xv = (word >> (v & 31)) & 1;
-        const double g = xv ? (double)y : -(double)y;
-        const float gv = (float)g;
-        if (gv > bv) {  // v ascends within a thread: strict '>' keeps the lowest node
-          bv = gv;
-          bi = v;
-          bg = g;
-          bx = xv;
+        // v ascends within a thread: strict '>' keeps the lowest node
+        if constexpr (std::is_same<GT, float>::value) {
+          const float gv = xv ? y : -y;
+          if (gv > bv) {
+            bv = gv;
+            bi = v;
+            bx = xv;
+          }
+        } else if constexpr (std::is_same<GT, int>::value) {
+          const int gi = xv ? y : -y;
+          if (gi > bint) {
+            bint = gi;
+            bi = v;
+            bx = xv;
+          }
+        } else {
+          const double g = xv ? y : -y;
+          const float gv = (float)g;
+          if (gv > bv) {
+            bv = gv;
+            bi = v;
+            bg = g;
+            bx = xv;
+          }
         }
       }
     }
@@ -211,6 +235,12 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
         }
       }
     }
+  }
+  if constexpr (std::is_same<GT, float>::value) {
+    bg = (double)bv;
+  } else if constexpr (std::is_same<GT, int>::value) {
+    bv = (float)bint;
+    bg = (double)bint;
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const unsigned long long key = bi >= 0 ? bkey(bv, bi, bx) : 0ull;
