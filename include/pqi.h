@@ -449,6 +449,18 @@ pqi_status pqi_tfim_jz_f32(const float* W, int n, double* J_eff, unsigned int* d
 pqi_status pqi_coo_to_dense(const int* rows, const int* cols, const float* vals, long long nnz,
                             int n, float* S, float* W, int* bad, void* stream);
 
+/* One batch of branch-and-bound frontier nodes of the exact solver
+ * (solve_maxcut_bnb.py:47-121, called from the loop of :128-199). fixed_t holds
+ * the nodes' assignments node-minor: entry i of node b at fixed_t[i * count + b]
+ * (-1 free, 0 / 1 fixed). W is the caller's n*n float32 matrix (upper triangle
+ * read). Per node, in the reference's summation order: ub[b] = the decoupled
+ * upper bound; state[b] = 0 when ub[b] <= best_value + 1e-9 (pruned), else 1 for a
+ * leaf with leaf_value[b] = its cut (is_spin_glass 0) or energy (1), else 2 with
+ * branch_var[b] = the first free variable of largest free-to-free |W| sum. */
+pqi_status pqi_bnb_eval(const float* W, int n, const int8_t* fixed_t, int count, double best_value,
+                        int is_spin_glass, double* ub, double* leaf_value, int* branch_var,
+                        int8_t* state, void* stream);
+
 /* Workspace bytes pqi_tfim_cdf needs. */
 size_t pqi_tfim_cdf_workspace_bytes(int n, int quality);
 

@@ -10,6 +10,9 @@ cover, each on one B200 with CUDA events on the launching stream:
           65,536 shots) and maxcut_tfim end to end on ER(1024, 0.5) at quality 2
   sparse  spin_glass_solver_sparse on G(16384, 0.01) N(0,1) against the dense
           solver on the same matrix
+  bnb     solve_maxcut_bnb (exact branch and bound) on 3-regular +-1 graphs,
+          n = 28 and 32, from a fixed warm start, with the reference's batch cap
+          of the build container (64) and with 4096 nodes per launch
 
 Usage: python profiles/run_row_legs.py [leg ...]  (default: all legs). One JSON
 line per measurement. Exits non-zero on a library error."""
@@ -170,7 +173,32 @@ def leg_sparse():
          note="same best_guess; host wall time per call, coordinate upload / W upload included")
 
 
-LEGS = {"double": leg_double, "gray": leg_gray, "tfim": leg_tfim, "sparse": leg_sparse}
+def leg_bnb():
+    import contextlib
+    import io
+    import re
+
+    from pyqrackising_b200 import solve_maxcut_bnb
+
+    warm = solve_maxcut_bnb(wl.regular_pm1_fast(12, seed=3), best_guess="0" * 12, verbose=False)
+    assert warm[4]
+    for n in (28, 32):
+        W = wl.regular_pm1_fast(n, seed=3)
+        rng = np.random.default_rng(1)
+        guess = "".join("1" if b else "0" for b in rng.random(n) < 0.5)
+        for cap in (64, 4096):
+            buf = io.StringIO()
+            t0 = time.perf_counter()
+            with contextlib.redirect_stdout(buf):
+                bits, cut, _, _, certified = solve_maxcut_bnb(W, best_guess=guess, verbose=True, batch_size=cap)
+            dt = time.perf_counter() - t0
+            m = re.search(r"Nodes explored: (\d+)\s+\|\s+Pruned: (\d+)", buf.getvalue())
+            emit(leg="bnb", graph=f"3-regular n={n} +-1", batch_size=cap, wall_s=round(dt, 3), cut=cut,
+                 certified=bool(certified), nodes=int(m.group(1)), pruned=int(m.group(2)),
+                 nodes_per_s=round(int(m.group(1)) / dt))
+
+
+LEGS = {"double": leg_double, "gray": leg_gray, "tfim": leg_tfim, "sparse": leg_sparse, "bnb": leg_bnb}
 
 if __name__ == "__main__":
     for name in sys.argv[1:] or list(LEGS):
