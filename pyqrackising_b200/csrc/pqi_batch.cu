@@ -137,17 +137,19 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   int bint = INT_MIN;
   constexpr int stride = 1024;  // 4 nodes x 256 threads
   // one group of four nodes v0 .. v0 + 3 with their weights of row k
+  // (v0 is a multiple of four: node v0 + i sits at fpos(v0) + 256 i)
   auto group = [&](int v0, const WT* w4) {
     if (k >= v0 && k < v0 + 4) c.bits[k >> 5] ^= 1u << (k & 31);
     const uint32_t word = c.bits[v0 >> 5];
+    GT* const g0 = c.g + fpos(v0);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int v = v0 + i;
       if (v < n) {
-        GT y = c.g[fpos(v)];
+        GT y = g0[256 * i];
         if (k >= 0) {
           y += coef * (GT)w4[i];
-          c.g[fpos(v)] = y;
+          g0[256 * i] = y;
         }
         const int xv = (word >> (v & 31)) & 1;
         // v ascends within a thread: strict '>' keeps the lowest node
