@@ -281,6 +281,12 @@ __device__ __forceinline__ int sample_mag(const double* cum, int len, double p) 
 constexpr int kWtsPitch = 33;  // doubles per row of a warp's weight table (32 lanes + 1)
 constexpr int kRowBatch = 16;  // row steps of 32 weights in flight per repulsion update
 
+// base^(-w) for a weight other than +-1, out of line: the unrolled update loop
+// stays small enough for the instruction cache
+__device__ __noinline__ double repulsion_factor(double lnb, float wv) {
+  return exp(-lnb * (double)wv);
+}
+
 __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
                                    const double* __restrict__ cum, int ncum, double base,
                                    int repel, uint64_t seed, uint64_t round, int shots,
@@ -295,7 +301,8 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
   double* wts = use_smem ? reinterpret_cast<double*>(smem) + (size_t)wib * (C * kWtsPitch)
                          : wglob + (size_t)(blockIdx.x * wpb + wib) * (C * kWtsPitch);
   const double lnb = log(base);
-  const double rep1 = exp(-lnb);  // repulsion factor of a unit weight
+  const double rep1 = exp(-lnb);  // repulsion factors of the weights +1 and -1
+  const double repm1 = exp(lnb);
   for (int s = blockIdx.x * wpb + wib; s < shots; s += gridDim.x * wpb) {
     const int m = sample_mag(cum, ncum, uniform(seed, round, (uint64_t)s, 0));
     const int node0 = s % n;
@@ -316,9 +323,19 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
     int node = node0;
     for (int j = 0; j <= picks; ++j) {
       if (j > 0) {
-        // bit_pick (util:711-724): p = sum(weights) * u, first i with p < running sum
-        double loc = 0.0;
-        for (int i = 0; i < C; ++i) loc += wts[i * kWtsPitch + lane];
+        // bit_pick (util:711-724): p = sum(weights) * u, first i with p < running sum.
+        // The lane's sum runs as four interleaved partial sums (independent
+        // adds instead of one chain of C).
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        int i = 0;
+        for (; i + 3 < C; i += 4) {
+          a0 += wts[i * kWtsPitch + lane];
+          a1 += wts[(i + 1) * kWtsPitch + lane];
+          a2 += wts[(i + 2) * kWtsPitch + lane];
+          a3 += wts[(i + 3) * kWtsPitch + lane];
+        }
+        for (; i < C; ++i) a0 += wts[i * kWtsPitch + lane];
+        const double loc = (a0 + a1) + (a2 + a3);
         double incl = loc;
         for (int o = 1; o < 32; o <<= 1) {
           const double y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
@@ -329,19 +346,25 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
         const unsigned hit = __ballot_sync(0xFFFFFFFFu, p < incl);
         int picked = 0;
         if (hit) {
+          // lane l's chunk holds the pick: the whole warp scans its C weights,
+          // 32 at a time (inclusive warp scan on top of the running sum)
           const int l = __ffs(hit) - 1;
-          if (lane == l) {
-            double run = incl - loc;
-            picked = v0;
-            for (int i = 0; i < C; ++i) {
-              run += wts[i * kWtsPitch + lane];
-              if (p < run) {
-                picked = v0 + i;
-                break;
-              }
+          double run = __shfl_sync(0xFFFFFFFFu, incl - loc, l);
+          picked = l * C;  // no prefix above p (rounding): the chunk's first node
+          for (int i0 = 0; i0 < C; i0 += 32) {
+            const int ii = i0 + lane;
+            double w = (ii < C) ? wts[ii * kWtsPitch + l] : 0.0;
+            for (int o = 1; o < 32; o <<= 1) {
+              const double y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+              if (lane >= o) w += y;
             }
+            const unsigned h2 = __ballot_sync(0xFFFFFFFFu, ii < C && p < run + w);
+            if (h2) {
+              picked = l * C + i0 + __ffs(h2) - 1;
+              break;
+            }
+            run += __shfl_sync(0xFFFFFFFFu, w, 31);
           }
-          picked = __shfl_sync(0xFFFFFFFFu, picked, l);
         }
         node = picked;
       }
@@ -364,7 +387,9 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
 #pragma unroll
           for (int u = 0; u < kRowBatch; ++u) {
             if (wv[u] != 0.0f)
-              wts[r * kWtsPitch + q] *= (wv[u] == 1.0f) ? rep1 : exp(-lnb * (double)wv[u]);
+              wts[r * kWtsPitch + q] *= (wv[u] == 1.0f)    ? rep1
+                                        : (wv[u] == -1.0f) ? repm1
+                                                           : repulsion_factor(lnb, wv[u]);
             q += dq;
             r += dr;
             if (r >= C) {
