@@ -114,3 +114,34 @@ def test_heuristic_warm_start_and_time_limit():
     assert certified and cut == pytest.approx(best)
     _, _, _, _, certified = solve_maxcut_bnb(W, best_guess="0" * n, verbose=False, time_limit=-1.0)
     assert certified is False
+
+
+def test_graph_input_and_tiny_graphs():
+    """nx.Graph input (nodes in graph order, missing weights read as 1.0) and
+    the reference's answers below three nodes (solve_maxcut_bnb.py:263-271)."""
+    import networkx as nx
+
+    from oracle import bnb_oracle as B
+    from pyqrackising_b200 import solve_maxcut_bnb
+
+    g = nx.Graph()
+    labels = ["a", "b", "c", "d", "e", "f", "g"]
+    g.add_nodes_from(labels)
+    for u, v, w in [("a", "b", 2.0), ("b", "c", None), ("c", "d", -1.0), ("d", "a", 3.0), ("e", "f", 1.5),
+                    ("f", "g", 2.5), ("g", "e", -0.5), ("a", "e", 1.0)]:
+        if w is None:
+            g.add_edge(u, v)
+        else:
+            g.add_edge(u, v, weight=w)
+    W = nx.to_numpy_array(g, nodelist=labels, weight="weight", nonedge=0.0, dtype=np.float32)
+    guess = "0101010"
+    bits, cut, (l, r), energy, certified = solve_maxcut_bnb(g, best_guess=guess, verbose=False, batch_size=4)
+    obits, ocut, oen, _ = B.solve(W, guess, False, 4)
+    assert certified and bits == obits and cut == pytest.approx(ocut) and energy == pytest.approx(oen)
+    assert sorted(l + r) == sorted(labels) and all(labels[i] in r for i, ch in enumerate(bits) if ch == "1")
+    assert solve_maxcut_bnb(np.zeros((0, 0), dtype=np.float32), verbose=False) == ("", 0, ([], []), 0, True)
+    assert solve_maxcut_bnb(np.zeros((1, 1), dtype=np.float32), verbose=False) == ("0", 0, ([0], []), 0, True)
+    pos = np.array([[0.0, 2.0], [2.0, 0.0]], dtype=np.float32)
+    assert solve_maxcut_bnb(pos, verbose=False) == ("01", 2.0, ([0], [1]), -2.0, True)
+    neg = -pos
+    assert solve_maxcut_bnb(neg, verbose=False) == ("00", 0, ([0, 1], []), -2.0, True)

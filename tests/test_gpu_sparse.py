@@ -130,3 +130,18 @@ def test_device_expansion_equals_the_host_expansion():
               None, D._ptr(W), D._ptr(bad), D.stream_ptr())
     assert int(bad.item()) == 1
     assert W.cpu().numpy().tolist() == [[0.0, 1.0, 0.0], [1.0, 0.0, 3.0], [0.0, 3.0, 0.0]]
+
+
+def test_graph_without_stored_entries():
+    """A 30-node sparse matrix with no stored entries: the device expansion
+    gives zero matrices and the solver returns a zero cut."""
+    from scipy.sparse import csr_matrix
+
+    from pyqrackising_b200 import spin_glass_solver_sparse
+    from pyqrackising_b200.sparse import sparse_to_device
+
+    G = csr_matrix((30, 30), dtype=np.float32)
+    _, W, S = sparse_to_device(G)
+    assert float(W.abs().sum()) == 0.0 and float(S.abs().sum()) == 0.0
+    bits, cut, (l, r), energy = spin_glass_solver_sparse(G, best_guess="0" * 30)
+    assert len(bits) == 30 and cut == 0.0 and energy == 0.0 and len(l) + len(r) == 30
