@@ -154,6 +154,53 @@ def solve_maxcut_bnb(
 ):
     nodes, G_m = as_matrix(G)
     G_m = np.asarray(G_m, dtype=np.float32)
+    return _solve(nodes, G_m, spin_glass_solver, best_guess, quality, shots, is_spin_glass, anneal_t,
+                  anneal_h, repulsion_base, is_maxcut_gpu, verbose, time_limit, gray_iterations,
+                  gray_seed_multiple, batch_size)
+
+
+def solve_maxcut_bnb_sparse(
+    G,
+    best_guess=None,
+    quality=None,
+    shots=None,
+    is_spin_glass=False,
+    anneal_t=None,
+    anneal_h=None,
+    repulsion_base=None,
+    is_maxcut_gpu=True,
+    verbose=True,
+    time_limit=None,
+    gray_iterations=None,
+    gray_seed_multiple=None,
+    batch_size=None,
+):
+    """The sparse-input B&B (pyqrackising/solve_maxcut_bnb_sparse.py:217-322):
+    an nx.Graph or a scipy sparse matrix of upper-triangular stored entries (the
+    reference's own layout, maxcut_tfim_util.py:533-542). Its bound, leaf and
+    score loops over the stored entries (:33-121) are the dense loops over
+    W = S + S^T, so the graph is expanded (on the device from 23 nodes) and the
+    dense B&B runs; the warm start is spin_glass_solver_sparse. The branching
+    score adds the same terms in another order (bit-equal for integer
+    weights). A matrix that also stores lower-triangle entries is read as
+    W = S + S^T throughout, as the sparse solver reads it."""
+    from .sparse import _dense_operands, spin_glass_solver_sparse
+
+    nodes, W, _ = _dense_operands(G)
+
+    def heuristic(_W, **kwargs):
+        return spin_glass_solver_sparse(G, **kwargs)
+
+    return _solve(nodes, W, heuristic, best_guess, quality, shots, is_spin_glass, anneal_t, anneal_h,
+                  repulsion_base, is_maxcut_gpu, verbose, time_limit, gray_iterations, gray_seed_multiple,
+                  batch_size)
+
+
+def _solve(nodes, W, heuristic, best_guess, quality, shots, is_spin_glass, anneal_t, anneal_h,
+           repulsion_base, is_maxcut_gpu, verbose, time_limit, gray_iterations, gray_seed_multiple, batch_size):
+    """solve_maxcut_bnb.py:253-321 on the dense matrix W (host array or device
+    tensor); `heuristic` is the warm-start solver, called as the reference
+    calls spin_glass_solver when best_guess is None."""
     n_qubits = len(nodes)
 
     if n_qubits < 3:
@@ -162,7 +209,7 @@ def solve_maxcut_bnb(
         if n_qubits == 1:
             return "0", 0, (nodes, []), 0, True
         if n_qubits == 2:
-            weight = G_m[0, 1]
+            weight = W[0, 1]
             if weight < 0.0:
                 return "00", 0, (nodes, []), weight, True
             return "01", weight, ([nodes[0]], [nodes[1]]), -weight, True
@@ -186,11 +233,11 @@ def solve_maxcut_bnb(
                 kwargs[key] = val
         kwargs["is_maxcut_gpu"] = is_maxcut_gpu
         t0 = time.monotonic()
-        bitstring, cut_value, _, energy_value = spin_glass_solver(G_m, is_spin_glass=is_spin_glass, **kwargs)
+        bitstring, cut_value, _, energy_value = heuristic(W, is_spin_glass=is_spin_glass, **kwargs)
         if verbose:
             print(f"Heuristic value: {cut_value:.6f}  ({time.monotonic()-t0:.3f}s)")
 
-    dg = D.DeviceGraph(G_m)
+    dg = D.DeviceGraph(W)
     best_theta = np.array([b == "1" for b in list(bitstring)], dtype=np.bool_)
     if is_spin_glass:
         if energy_value is None:

@@ -6,17 +6,21 @@ importing the reference in the build container (PYTHONPATH=/root/reference):
 Writes tests/golden/golden_bnb.npz: per case the dense float32 matrix W, the
 warm start (best_guess bit string), the objective (cut or spin glass), the
 reference's returned bit string, cut, energy and certified flag
-(solve_maxcut_bnb.py:208-321, run with verbose=False), and the batch cap the
-reference used here (os.cpu_count() ** 2, which fixes its traversal order)."""
+(solve_maxcut_bnb.py:208-321, run with verbose=False), the same for the sparse
+solver on the upper-triangular CSR of W (solve_maxcut_bnb_sparse.py:217-322,
+keys *_sparse_*), and the batch cap the reference used here (os.cpu_count() ** 2,
+which fixes its traversal order)."""
 
 import importlib
 import os
 import sys
 
 import numpy as np
+from scipy.sparse import csr_matrix
 
 sys.path.insert(0, "/root/reference")
 bnb = importlib.import_module("pyqrackising.solve_maxcut_bnb")
+bnbs = importlib.import_module("pyqrackising.solve_maxcut_bnb_sparse")
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 rng = np.random.default_rng(41)
@@ -64,4 +68,11 @@ for name, W, spin in cases:
     out[f"{name}_energy"] = np.float64(energy)
     out[f"{name}_certified"] = np.int64(bool(certified))
     print(name, bits, cut, energy, certified)
+    sb, sc, _, se, scert = bnbs.solve_maxcut_bnb_sparse(csr_matrix(np.triu(W, 1)), best_guess=guess,
+                                                         is_spin_glass=spin, verbose=False)
+    out[f"{name}_sparse_bits"] = np.array(sb)
+    out[f"{name}_sparse_cut"] = np.float64(sc)
+    out[f"{name}_sparse_energy"] = np.float64(se)
+    out[f"{name}_sparse_certified"] = np.int64(bool(scert))
+    print(name, "sparse", sb, sc, se, scert)
 np.savez_compressed(os.path.join(HERE, "golden_bnb.npz"), **out)

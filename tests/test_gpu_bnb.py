@@ -145,3 +145,31 @@ def test_graph_input_and_tiny_graphs():
     assert solve_maxcut_bnb(pos, verbose=False) == ("01", 2.0, ([0], [1]), -2.0, True)
     neg = -pos
     assert solve_maxcut_bnb(neg, verbose=False) == ("00", 0, ([0, 1], []), -2.0, True)
+
+
+def test_sparse_input_matches_the_reference_sparse_solver():
+    """solve_maxcut_bnb_sparse on the upper-triangular CSR of each fixture
+    graph (and on the same graph as nx input) returns the reference sparse
+    solver's bit strings, values and certificates."""
+    import networkx as nx
+    from scipy.sparse import csr_matrix
+
+    from pyqrackising_b200 import solve_maxcut_bnb_sparse
+
+    z, names = _cases()
+    cap = int(z["batch_cap"])
+    for name in names:
+        W = z[f"{name}_W"]
+        spin = bool(z[f"{name}_spin"])
+        guess = str(z[f"{name}_guess"])
+        g = nx.Graph()
+        g.add_nodes_from(range(W.shape[0]))
+        for a, b in zip(*np.nonzero(np.triu(W, 1))):
+            g.add_edge(int(a), int(b), weight=float(W[a, b]))
+        for G in (csr_matrix(np.triu(W, 1)), g):
+            bits, cut, _, energy, certified = solve_maxcut_bnb_sparse(
+                G, best_guess=guess, is_spin_glass=spin, verbose=False, batch_size=cap)
+            assert bits == str(z[f"{name}_sparse_bits"]), name
+            assert cut == pytest.approx(float(z[f"{name}_sparse_cut"]), rel=1e-6, abs=1e-6), name
+            assert energy == pytest.approx(float(z[f"{name}_sparse_energy"]), rel=1e-6, abs=1e-6), name
+            assert certified == bool(z[f"{name}_sparse_certified"])
