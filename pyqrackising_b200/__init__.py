@@ -7,6 +7,7 @@ Public API (same signatures and return tuples as the reference):
                     anneal_t, anneal_h, repulsion_base, is_log, gray_iterations,
                     gray_seed_multiple, bp_scale, bp_damping)
   maxcut_tfim_sparse / spin_glass_solver_sparse (CSR or graph input)
+  spin_glass_solver_hybrid (dense maxcut_tfim seed, then the sparse solver)
   solve_maxcut_bnb(G, best_guess, quality, shots, is_spin_glass, anneal_t, anneal_h,
                    repulsion_base, is_maxcut_gpu, verbose, time_limit,
                    gray_iterations, gray_seed_multiple[, batch_size])
@@ -19,7 +20,8 @@ CUDA behind the C ABI in include/pqi.h); there is no CPU fallback.
 from .maxcut_tfim import maxcut_tfim
 from .spin_glass_solver import spin_glass_solver
 from .solve_maxcut_bnb import solve_maxcut_bnb, solve_maxcut_bnb_sparse
-from .sparse import maxcut_tfim_sparse, spin_glass_solver_sparse
+from .sparse import maxcut_tfim_sparse, spin_glass_solver_hybrid, spin_glass_solver_sparse
 
 __all__ = ["maxcut_tfim", "spin_glass_solver", "maxcut_tfim_sparse", "spin_glass_solver_sparse",
+           "spin_glass_solver_hybrid",
            "solve_maxcut_bnb", "solve_maxcut_bnb_sparse"]

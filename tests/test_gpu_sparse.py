@@ -145,3 +145,30 @@ def test_graph_without_stored_entries():
     assert float(W.abs().sum()) == 0.0 and float(S.abs().sum()) == 0.0
     bits, cut, (l, r), energy = spin_glass_solver_sparse(G, best_guess="0" * 30)
     assert len(bits) == 30 and cut == 0.0 and energy == 0.0 and len(l) + len(r) == 30
+
+
+def test_hybrid_is_the_dense_seed_then_the_sparse_solver():
+    """spin_glass_solver_hybrid (spin_glass_solver_hybrid.py:7-46): with the
+    sampler's seed fixed it returns what the two steps return run by hand;
+    anything but an nx.Graph is refused, as in the reference."""
+    import importlib
+
+    import networkx as nx
+
+    from pyqrackising_b200 import spin_glass_solver_hybrid, spin_glass_solver_sparse
+
+    MT = importlib.import_module("pyqrackising_b200.maxcut_tfim")
+    rng = np.random.default_rng(9)
+    g = nx.random_regular_graph(3, 40, seed=4)
+    for u, v in g.edges():
+        g[u][v]["weight"] = float(rng.choice([-1.0, 1.0]))
+    for spin in (True, False):
+        MT.set_seed(5)
+        got = spin_glass_solver_hybrid(g, quality=2, is_spin_glass=spin)
+        MT.set_seed(5)
+        guess, _, _ = MT.maxcut_tfim(g, quality=2, is_spin_glass=spin)
+        want = spin_glass_solver_sparse(g, best_guess=guess, is_spin_glass=spin)
+        MT.set_seed(None)
+        assert got == want
+    with pytest.raises(TypeError):
+        spin_glass_solver_hybrid(np.zeros((30, 30), dtype=np.float32))
