@@ -240,6 +240,15 @@ __global__ void __launch_bounds__(256) cluster_ascent_kernel(
         const unsigned long long cb = warp_max_key(ck);
         const uint32_t src = __ballot_sync(0xFFFFFFFFu, ck == cb && cb != 0ull);
         const double cbg = __shfl_sync(0xFFFFFFFFu, cgv, src ? __ffs(src) - 1 : 0);
+        // the next row is one of the C CTAs' candidates: pull this CTA's
+        // candidate row into L2 while the exchange is in flight (a hint only;
+        // a row is ld * sizeof(WT) bytes, 16-byte aligned, inside W)
+        if (lane == 0 && cb != 0ull && key_gain(cb) > 0.0f) {
+          const WT* cand = W + (size_t)key_node(cb) * G.ld;
+          asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(cand),
+                       "r"((uint32_t)((size_t)G.ld * sizeof(WT)))
+                       : "memory");
+        }
         if (lane < C) {
           // this CTA's best into slot [rank] of CTA `lane`, counted on its bar[par]
           uint32_t raddr, rbar;
