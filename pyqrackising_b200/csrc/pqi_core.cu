@@ -288,10 +288,10 @@ __global__ void __launch_bounds__(256) double_kernel(const WT* __restrict__ Wp, 
       int l = k + 1 + threadIdx.x;
       uint32_t i = base + (uint32_t)l;
       uint32_t t = i % geo.G, j = i / geo.G;
-#pragma unroll 4
-      for (; l < n; l += blockDim.x) {
-        const double w = (double)row[l];
-        const double d = gk + __ldg(g64 + l) - ((get_bit32(theta, l) == xk) ? 2.0 * w : -2.0 * w);
+      // one pair: value from the gains, then its selection key
+      auto pair = [&](WT wr, double gl, uint32_t word, int ll) {
+        const double w = (double)wr;
+        const double d = gk + gl - ((((word >> (ll & 31)) & 1u) == (uint32_t)xk) ? 2.0 * w : -2.0 * w);
         float v = (float)d;
         if (spin) v *= 2.0f;
         uint64_t kk;
@@ -311,7 +311,23 @@ __global__ void __launch_bounds__(256) double_kernel(const WT* __restrict__ Wp, 
           t -= geo.G;
           ++j;
         }
+      };
+      // four steps' loads in flight before any is used
+      const int bd = blockDim.x;
+      for (; l + 3 * bd < n; l += 4 * bd) {
+        WT wr[4];
+        double gl[4];
+        uint32_t wd[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          wr[u] = row[l + u * bd];
+          gl[u] = __ldg(g64 + l + u * bd);
+          wd[u] = __ldg(theta + ((l + u * bd) >> 5));
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) pair(wr[u], gl[u], wd[u], l + u * bd);
       }
+      for (; l < n; l += bd) pair(row[l], __ldg(g64 + l), __ldg(theta + (l >> 5)), l);
     }
   }
   best = block_max_u64(best, scratch);
@@ -637,8 +653,20 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     gains64 = g;
   }
   PQI_TRY(cudaMemsetAsync(key, 0, sizeof(unsigned long long), s));
-  const int grid = std::max(1, std::min(n >> 1, 148 * 8));
+  // one resident wave of blocks (a partial second wave would idle most SMs)
+  static int resident[2][2] = {{0, 0}, {0, 0}};
   const bool tab = geo.G <= (uint32_t)kDoubleTab;
+  const int i8 = w->kind == PQI_W_I8 ? 1 : 0;
+  if (!resident[i8][tab]) {
+    int dev = 0, sms = 0, per_sm = 0;
+    PQI_TRY(cudaGetDevice(&dev));
+    PQI_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const void* fn = i8 ? (tab ? (const void*)double_kernel<int8_t, true> : (const void*)double_kernel<int8_t, false>)
+                        : (tab ? (const void*)double_kernel<float, true> : (const void*)double_kernel<float, false>);
+    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
+    resident[i8][tab] = std::max(1, sms * std::max(1, per_sm));
+  }
+  const int grid = std::max(1, std::min(n >> 1, resident[i8][tab]));
   if (w->kind == PQI_W_I8) {
     if (tab)
       double_kernel<int8_t, true><<<grid, 256, 0, s>>>(w->W_i8, w->ld, n, theta, gains64,
