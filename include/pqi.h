@@ -485,6 +485,25 @@ pqi_status pqi_tfim_sample(const float* W, int n, const double* cum, double repu
                            uint64_t seed, uint64_t round, int shots, uint32_t* theta_out,
                            void* workspace, size_t workspace_bytes, void* stream);
 
+/* pqi_tfim_sample with the nonzero entries of W's rows as lists (row r's
+ * columns adj_col[adj_ptr[r] .. adj_ptr[r+1]) ascending, values adj_val, from
+ * pqi_tfim_adj_count / pqi_tfim_adj_fill): a repulsion update
+ * (maxcut_tfim.py:37-45) walks the picked node's list instead of scanning its
+ * row. The same multiplications in the same order: the same draws, bit for bit. */
+pqi_status pqi_tfim_sample_adj(const float* W, int n, const long long* adj_ptr, const int* adj_col,
+                               const float* adj_val, const double* cum, double repulsion_base,
+                               uint64_t seed, uint64_t round, int shots, uint32_t* theta_out,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
+/* Nonzero count of each row of the n*n float32 W (count: n int64, device). */
+pqi_status pqi_tfim_adj_count(const float* W, int n, long long* count, void* stream);
+
+/* Row lists of W's nonzero entries in column order: row r at adj_ptr[r] (n + 1
+ * int64, the exclusive prefix sum of the counts), columns into adj_col, values
+ * into adj_val. */
+pqi_status pqi_tfim_adj_fill(const float* W, int n, const long long* adj_ptr, int* adj_col,
+                             float* adj_val, void* stream);
+
 /* ---------------------------------------------------------------------------
  * Objectives, packing
  * -------------------------------------------------------------------------*/

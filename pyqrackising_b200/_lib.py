@@ -117,6 +117,9 @@ SIGNATURES = {
     "pqi_tfim_cdf": (_i, [_vp, _vp, _i, _i, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _sz, _vp]),
     "pqi_tfim_sample_workspace_bytes": (_sz, [_i]),
     "pqi_tfim_sample": (_i, [_vp, _i, _vp, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, _i, _vp, _vp, _sz, _vp]),
+    "pqi_tfim_sample_adj": (_i, [_vp, _i, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_uint64, ctypes.c_uint64, _i, _vp, _vp, _sz, _vp]),
+    "pqi_tfim_adj_count": (_i, [_vp, _i, _vp, _vp]),
+    "pqi_tfim_adj_fill": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
     "pqi_exact_search": (_i, [_vp, _i, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_rescore_fp64": (_i, [_WP, _vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_pack_bits": (_i, [_vp, _i, _i, _vp, _vp]),

@@ -287,11 +287,16 @@ __device__ __noinline__ double repulsion_factor(double lnb, float wv) {
   return exp(-lnb * (double)wv);
 }
 
+// adj_ptr / adj_col / adj_val (nullable): the nonzero entries of each row of W
+// in column order; when given, a repulsion update walks the picked node's
+// list instead of scanning its dense row (the same multiplications).
 __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
                                    const double* __restrict__ cum, int ncum, double base,
                                    int repel, uint64_t seed, uint64_t round, int shots,
                                    uint32_t* __restrict__ theta_out, double* __restrict__ wglob,
-                                   int use_smem) {
+                                   int use_smem, const long long* __restrict__ adj_ptr,
+                                   const int* __restrict__ adj_col,
+                                   const float* __restrict__ adj_val) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -372,7 +377,18 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
       __syncwarp();
       if (lane == (node / C)) wts[(node - lane * C) * kWtsPitch + lane] = 0.0;
       __syncwarp();
-      if (j < picks && repel) {
+      if (j < picks && repel && adj_ptr) {
+        // the picked node's nonzero weights, 32 list entries per step
+        const long long e1 = adj_ptr[node + 1];
+        for (long long e = adj_ptr[node] + lane; e < e1; e += 32) {
+          const int v = adj_col[e];
+          const float wv = adj_val[e];
+          const int q = v / C;
+          wts[(v - q * C) * kWtsPitch + q] *= (wv == 1.0f)    ? rep1
+                                              : (wv == -1.0f) ? repm1
+                                                              : repulsion_factor(lnb, wv);
+        }
+      } else if (j < picks && repel) {
         // the row in node order, 32 consecutive weights per step (coalesced),
         // kRowBatch steps loaded before any is applied (the weight table may
         // be global memory, so loads would otherwise wait behind the stores);
@@ -409,6 +425,42 @@ __global__ void tfim_sample_kernel(const float* __restrict__ W, int n,
       if (lane == 0) out[w] = bits;
     }
     __syncwarp();
+  }
+}
+
+// Nonzero counts of W's rows (warp per row).
+__global__ void tfim_adj_count_kernel(const float* __restrict__ W, int n, long long* __restrict__ count) {
+  const int lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
+    const float* row = W + (size_t)r * n;
+    int c = 0;
+    for (int v0 = 0; v0 < n; v0 += 32) {
+      const int v = v0 + lane;
+      c += __popc(__ballot_sync(0xFFFFFFFFu, v < n && row[v] != 0.0f));
+    }
+    if (lane == 0) count[r] = c;
+  }
+}
+
+// Row lists in column order at adj_ptr[r] (warp per row, ballot compaction).
+__global__ void tfim_adj_fill_kernel(const float* __restrict__ W, int n,
+                                     const long long* __restrict__ adj_ptr, int* __restrict__ adj_col,
+                                     float* __restrict__ adj_val) {
+  const int lane = threadIdx.x & 31;
+  for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < n; r += (gridDim.x * blockDim.x) >> 5) {
+    const float* row = W + (size_t)r * n;
+    long long at = adj_ptr[r];
+    for (int v0 = 0; v0 < n; v0 += 32) {
+      const int v = v0 + lane;
+      const float w = v < n ? row[v] : 0.0f;
+      const unsigned nz = __ballot_sync(0xFFFFFFFFu, w != 0.0f);
+      if (w != 0.0f) {
+        const long long e = at + __popc(nz & ((1u << lane) - 1u));
+        adj_col[e] = v;
+        adj_val[e] = w;
+      }
+      at += __popc(nz);
+    }
   }
 }
 
@@ -494,9 +546,10 @@ size_t pqi_tfim_sample_workspace_bytes(int n) {
   return (size_t)148 * 16 * kWtsPitch * C * sizeof(double) + 4096;
 }
 
-pqi_status pqi_tfim_sample(const float* W, int n, const double* cum, double repulsion_base,
-                           uint64_t seed, uint64_t round, int shots, uint32_t* theta_out,
-                           void* workspace, size_t workspace_bytes, void* stream) {
+static pqi_status tfim_sample_impl(const float* W, int n, const double* cum, double repulsion_base,
+                                   uint64_t seed, uint64_t round, int shots, uint32_t* theta_out,
+                                   void* workspace, size_t workspace_bytes, void* stream,
+                                   const long long* adj_ptr, const int* adj_col, const float* adj_val) {
   PQI_CHECK_ARG(W && cum && theta_out && n >= 3 && shots > 0);
   cudaStream_t s = as_stream(stream);
   const int C = (n + 31) / 32;
@@ -527,8 +580,42 @@ pqi_status pqi_tfim_sample(const float* W, int n, const double* cum, double repu
     PQI_CHECK_ARG(wglob);
   }
   tfim_sample_kernel<<<grid, 32 * wpb, smem, s>>>(W, n, cum, n - 1, repulsion_base, repel, seed,
-                                                   round, shots, theta_out, wglob, use_smem);
+                                                   round, shots, theta_out, wglob, use_smem,
+                                                   adj_ptr, adj_col, adj_val);
   PQI_LAUNCHED("tfim_sample_kernel");
+  return PQI_OK;
+}
+
+pqi_status pqi_tfim_sample(const float* W, int n, const double* cum, double repulsion_base,
+                           uint64_t seed, uint64_t round, int shots, uint32_t* theta_out,
+                           void* workspace, size_t workspace_bytes, void* stream) {
+  return tfim_sample_impl(W, n, cum, repulsion_base, seed, round, shots, theta_out, workspace,
+                          workspace_bytes, stream, nullptr, nullptr, nullptr);
+}
+
+pqi_status pqi_tfim_sample_adj(const float* W, int n, const long long* adj_ptr, const int* adj_col,
+                               const float* adj_val, const double* cum, double repulsion_base,
+                               uint64_t seed, uint64_t round, int shots, uint32_t* theta_out,
+                               void* workspace, size_t workspace_bytes, void* stream) {
+  PQI_CHECK_ARG(adj_ptr && (adj_col || !adj_val) && (adj_val || !adj_col));
+  return tfim_sample_impl(W, n, cum, repulsion_base, seed, round, shots, theta_out, workspace,
+                          workspace_bytes, stream, adj_ptr, adj_col, adj_val);
+}
+
+pqi_status pqi_tfim_adj_count(const float* W, int n, long long* count, void* stream) {
+  PQI_CHECK_ARG(W && count && n > 0);
+  const int blocks = (int)std::min<long long>(((long long)n + 7) / 8, 148 * 16);
+  tfim_adj_count_kernel<<<blocks, 256, 0, as_stream(stream)>>>(W, n, count);
+  PQI_LAUNCHED("tfim_adj_count_kernel");
+  return PQI_OK;
+}
+
+pqi_status pqi_tfim_adj_fill(const float* W, int n, const long long* adj_ptr, int* adj_col,
+                             float* adj_val, void* stream) {
+  PQI_CHECK_ARG(W && adj_ptr && n > 0);
+  const int blocks = (int)std::min<long long>(((long long)n + 7) / 8, 148 * 16);
+  tfim_adj_fill_kernel<<<blocks, 256, 0, as_stream(stream)>>>(W, n, adj_ptr, adj_col, adj_val);
+  PQI_LAUNCHED("tfim_adj_fill_kernel");
   return PQI_OK;
 }
 

@@ -190,15 +190,66 @@ def hamming_cdf(dg: D.DeviceGraph, quality: int, anneal_t: float, anneal_h: floa
     return J_eff, degrees, cum
 
 
-def sample_batch(dg: D.DeviceGraph, cum, shots: int, repulsion_base: float, seed: int, round_: int, out=None):
+ADJ_MAX_FILL = 0.25  # row lists pay off below this fraction of nonzero entries
+ADJ_MAX_BYTES = 4 << 30
+
+
+def row_lists(dg: D.DeviceGraph):
+    """The nonzero entries of W's rows as device lists (ptr int64[n+1], col
+    int32, val float32), built once per prepared graph; None when W is too
+    dense for lists to beat the row scan."""
+    if getattr(dg, "_row_lists", False) is not False:
+        return dg._row_lists
+    n = dg.n
+    count = torch.empty(n, dtype=torch.int64, device=dg.device)
+    _lib.call("pqi_tfim_adj_count", D._ptr(dg.W), n, D._ptr(count), dg.sp())
+    counts = count.cpu().numpy()
+    nnz = int(counts.sum())
+    lists = None
+    if nnz <= ADJ_MAX_FILL * n * n and nnz * 8 <= ADJ_MAX_BYTES:
+        ptr = np.zeros(n + 1, dtype=np.int64)
+        np.cumsum(counts, out=ptr[1:])
+        ptr_d = torch.from_numpy(ptr).to(dg.device)
+        col = torch.empty(max(nnz, 1), dtype=torch.int32, device=dg.device)
+        val = torch.empty(max(nnz, 1), dtype=torch.float32, device=dg.device)
+        _lib.call("pqi_tfim_adj_fill", D._ptr(dg.W), n, D._ptr(ptr_d), D._ptr(col), D._ptr(val), dg.sp())
+        lists = (ptr_d, col, val)
+    dg._row_lists = lists
+    return lists
+
+
+def sample_batch(dg: D.DeviceGraph, cum, shots: int, repulsion_base: float, seed: int, round_: int, out=None,
+                 lists="auto"):
     """One round of shot_loop (maxcut_tfim.py:139-145) on the device: `shots`
-    candidates as packed words [shots, ceil(n/32)]."""
+    candidates as packed words [shots, ceil(n/32)]. Graphs with few nonzero
+    weights per row use row lists for the repulsion updates (`lists`: "auto",
+    or False for the row scan; both give the same draws)."""
     n = dg.n
     lib = _lib.load()
     if out is None:
         out = torch.empty(shots * dg.n32 + 1, dtype=torch.int32, device=dg.device)
         out[-1] = 0  # spare word (single-row 64-bit view), never written by the sampler
     ws = dg.ws.get(lib.pqi_tfim_sample_workspace_bytes(n))
+    rl = row_lists(dg) if lists == "auto" else None
+    if rl is not None:
+        _lib.call(
+            "pqi_tfim_sample_adj",
+            D._ptr(dg.W),
+            n,
+            D._ptr(rl[0]),
+            D._ptr(rl[1]),
+            D._ptr(rl[2]),
+            D._ptr(cum),
+            float(repulsion_base),
+            ctypes.c_uint64(seed),
+            ctypes.c_uint64(round_),
+            int(shots),
+            D._ptr(out),
+            ws[0],
+            ws[1],
+            dg.sp(),
+        )
+        return out
     _lib.call(
         "pqi_tfim_sample",
         D._ptr(dg.W),

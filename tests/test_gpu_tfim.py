@@ -143,3 +143,28 @@ def test_maxcut_tfim_end_to_end_spin_glass():
         first = dg.unpack(buf, rows=shots)
         assert e >= max(O.compute_energy(b, W) for b in first) - 1e-9
     MT.set_seed(None)
+
+
+def test_row_lists_give_the_same_draws():
+    """The repulsion update over row lists (pqi_tfim_sample_adj) makes the
+    same multiplications as the row scan: identical batches on a 3-regular
+    graph, a sparse graph with general float weights (the out-of-line factor)
+    and a graph with a nonzero diagonal; a dense graph keeps the row scan."""
+    from pyqrackising_b200 import workloads as wl
+
+    d = load_golden("tfim")
+    rng = np.random.default_rng(3)
+    U = np.triu(np.where(rng.random((300, 300)) < 0.03, rng.standard_normal((300, 300)), 0.0), 1)
+    Wf = (U + U.T).astype(np.float32)
+    Wd = Wf.copy()
+    np.fill_diagonal(Wd, 0.5)
+    for W in (d["c1_W"], wl.regular_pm1_fast(1000, seed=2), Wf, Wd):
+        dg = _dg(W)
+        _, _, cum = MT.hamming_cdf(dg, 4, 8.0, 8.0)
+        assert MT.row_lists(dg) is not None
+        for rnd in (0, 3):
+            a = MT.sample_batch(dg, cum, 4096, 5.0, seed=11, round_=rnd, lists=False)
+            b = MT.sample_batch(dg, cum, 4096, 5.0, seed=11, round_=rnd)
+            assert torch.equal(a, b)
+    dense = _dg(np.ones((200, 200), dtype=np.float32) - np.eye(200, dtype=np.float32))
+    assert MT.row_lists(dense) is None
