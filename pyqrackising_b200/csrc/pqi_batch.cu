@@ -666,8 +666,10 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   const int groups = (max_n + 1023) / 1024;  // groups of four per thread
   // float32 fields beyond four groups: four more groups per pass staged in
   // shared memory (16 KB), all of SK n = 8192's row in flight per flip
-  const bool staged = f32 && !i8 && groups > 4 && !g_batch_no_stage;
-  const size_t smem_all = smem + (staged ? (size_t)kStageGroups * 256 * 4 * sizeof(float) : 0);
+  // (staging is skipped where its buffer would not fit: every row group in registers)
+  const size_t stage_bytes = (size_t)kStageGroups * 256 * 4 * sizeof(float);
+  const bool staged = f32 && !i8 && groups > 4 && !g_batch_no_stage && smem + stage_bytes <= 200 * 1024;
+  const size_t smem_all = smem + (staged ? stage_bytes : 0);
   PQI_CHECK_ARG(smem_all <= 200 * 1024);
   static int num_sms = 0;
   if (!num_sms) {
