@@ -331,6 +331,20 @@ pqi_status pqi_batch_search_f32(const void* graphs, int num_graphs, const int* t
                                 double* best_values, unsigned long long* flips_total,
                                 int* status, void* stream);
 
+/* pqi_batch_search (float32_fields 0) or pqi_batch_search_f32 (1) with the
+ * CTA size given: threads_per_task 256 (those entry points' size) or 128 (twice
+ * the resident tasks per SM at the same registers per thread; for graphs of up
+ * to about a thousand nodes). Same results for either size. No reference
+ * counterpart (batched form of spin_glass_solver.py:603-717). */
+pqi_status pqi_batch_search_cta(const void* graphs, int num_graphs, const int* task_graph,
+                                const uint32_t* init_states, int words_pitch, int tasks,
+                                int max_n, int kind, int is_spin_glass, int rounds, int kick,
+                                int flip_budget, uint64_t seed, const double* kick_cdf,
+                                const long long* cdf_offset, uint32_t* best_states,
+                                double* best_values, unsigned long long* flips_total,
+                                int* status, int threads_per_task, int float32_fields,
+                                void* stream);
+
 /* Tuning / cross-check knob (no reference counterpart): on (default) lets
  * pqi_batch_search_f32 (float32 local fields) stage four row groups per thread
  * in shared memory with cp.async for graphs of more than 4096 nodes; off keeps

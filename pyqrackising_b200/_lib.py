@@ -98,6 +98,7 @@ SIGNATURES = {
     "pqi_mpnn_transpose64": (_i, [_vp, _i, _i, _vp, _i, _vp]),
     "pqi_mpnn_adj_gemm": (_i, [_vp, _i, _i, _vp, _i, ctypes.c_float, _vp, _vp, _i, _vp]),
     "pqi_batch_search_f32": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pqi_batch_search_cta": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "pqi_batch_search_warp": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "pqi_cluster_ascent": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp]),
     "pqi_mpnn_gemm": (_i, [_i, _i, _i, _i, _i, ctypes.c_float, _vp, _i, _vp, _i, ctypes.c_float, _vp, _vp, _i, _vp, _i, _vp]),

@@ -46,12 +46,13 @@ __device__ __forceinline__ double bunif(uint64_t seed, uint64_t a, uint64_t b) {
   return (double)(h >> 11) * (1.0 / 9007199254740992.0);
 }
 
-// Shared-memory position of node v's field (256-thread CTAs): node
-// v = 4 t + 1024 j + i (thread t's group j, lane i of the group) sits at
-// (4 j + i) * 256 + t, so a warp's accesses in the flip pass are contiguous.
-// Holds ceil(n / 1024) * 1024 entries.
+// Shared-memory position of node v's field in a CTA of BT threads (BT a power
+// of two): node v = 4 t + 4 BT j + i (thread t's group j, lane i of the group)
+// sits at (4 j + i) * BT + t, so a warp's accesses in the flip pass are
+// contiguous. Holds ceil(n / (4 BT)) * 4 BT entries.
+template <int BT>
 __device__ __forceinline__ int fpos(int v) {
-  return (((v >> 10) << 2) + (v & 3)) * 256 + ((v >> 2) & 255);
+  return (((v / (4 * BT)) << 2) + (v & 3)) * BT + ((v >> 2) & (BT - 1));
 }
 
 template <typename WT, typename GT>
@@ -60,7 +61,7 @@ struct TaskCtx {
   int n, ld;
   GT* g;  // local fields y = W x
   uint32_t* bits;
-  WT* stage;  // staged row groups (kStageGroups x 256 threads x 4 weights), or null
+  WT* stage;  // staged row groups (kStageGroups x threads x 4 weights), or null
 };
 
 // Row groups per thread that the staged form copies with cp.async (no
@@ -109,7 +110,7 @@ __device__ __forceinline__ unsigned long long bmax_key(unsigned long long key) {
 // the gain of node v is g_v = x_v y_v, and flipping node k changes every
 // field by y_v -= 2 x_k W_kv (W's prepared copy has a zero diagonal, so y_k is
 // unchanged). One fused pass per flip, one CTA barrier: each thread owns
-// groups of four consecutive nodes v = 4 t + 1024 j + i, loads CH groups of
+// groups of four consecutive nodes v = 4 t + 4 BT j + i, loads CH groups of
 // row k at once (float4 / char4), updates their fields, toggles bit k if it
 // owns k (the only writer of that bit; the other nodes of the word are read
 // by their own threads only), and folds the new gains into a key (float gain,
@@ -118,7 +119,7 @@ __device__ __forceinline__ unsigned long long bmax_key(unsigned long long key) {
 // itself, so the next pass starts without a second barrier (a warp can be at
 // most one pass ahead of another, which writes the other slot array).
 // k < 0: no flip, only the selection. Returns the key and the exact gain.
-template <typename WT, typename GT, int CH, bool STG = false>
+template <typename WT, typename GT, int CH, bool STG, int BT>
 __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k, int xk,
                                                 unsigned long long (*red_key)[8],
                                                 double (*red_g)[8], int par,
@@ -135,21 +136,21 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   // (exact in float below 2^24, more than 127 x the largest n); double fields
   // round each gain to float once.
   int bint = INT_MIN;
-  constexpr int stride = 1024;  // 4 nodes x 256 threads
+  constexpr int stride = 4 * BT;  // 4 nodes x BT threads
   // one group of four nodes v0 .. v0 + 3 with their weights of row k
-  // (v0 is a multiple of four: node v0 + i sits at fpos(v0) + 256 i)
+  // (v0 is a multiple of four: node v0 + i sits at fpos(v0) + BT i)
   auto group = [&](int v0, const WT* w4) {
     if (k >= v0 && k < v0 + 4) c.bits[k >> 5] ^= 1u << (k & 31);
     const uint32_t word = c.bits[v0 >> 5];
-    GT* const g0 = c.g + fpos(v0);
+    GT* const g0 = c.g + fpos<BT>(v0);
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int v = v0 + i;
       if (v < n) {
-        GT y = g0[256 * i];
+        GT y = g0[BT * i];
         if (k >= 0) {
           y += coef * (GT)w4[i];
-          g0[256 * i] = y;
+          g0[BT * i] = y;
         }
         const int xv = (word >> (v & 31)) & 1;
         // v ascends within a thread: strict '>' keeps the lowest node
@@ -191,7 +192,7 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
         for (int j = 0; j < kStageGroups; ++j) {
           const int v = base + (CH + j) * stride;
           if (v < n)
-            cp_async16(c.stage + (size_t)(j * 256 + threadIdx.x) * 4, row + v,
+            cp_async16(c.stage + (size_t)(j * BT + threadIdx.x) * 4, row + v,
                        (n - v) >= 4 ? 16 : (n - v) * (int)sizeof(WT));
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
@@ -230,7 +231,7 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
           WT w4[4] = {(WT)0, (WT)0, (WT)0, (WT)0};
           if (k >= 0) {
             const float4 t =
-                *reinterpret_cast<const float4*>(c.stage + (size_t)(j * 256 + threadIdx.x) * 4);
+                *reinterpret_cast<const float4*>(c.stage + (size_t)(j * BT + threadIdx.x) * 4);
             w4[0] = t.x; w4[1] = t.y; w4[2] = t.z; w4[3] = t.w;
           }
           group(v0, w4);
@@ -265,8 +266,10 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
 // STG (float32 fields only): each flip pass also stages kStageGroups row
 // groups per thread through cp.async, so a pass of SK n = 8192 has its whole
 // 32 KB row in flight at once instead of in two register chunks.
-template <typename WT, int CH, bool F32, bool STG = false>
-__global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
+// BT: threads per CTA (256; 128 for small graphs: twice the resident tasks per
+// SM, at the same registers per thread).
+template <typename WT, int CH, bool F32, bool STG, int BT>
+__global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_kernel(
     const BatchGraph* __restrict__ graphs, const int* __restrict__ task_graph,
     const uint32_t* __restrict__ init_states, int words_pitch, int tasks, int spin, int rounds,
     int kick, int flip_budget, uint64_t seed, const double* __restrict__ kick_cdf,
@@ -289,7 +292,8 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
     c.bits = reinterpret_cast<uint32_t*>(smem);
     c.g = reinterpret_cast<GT*>(smem + (((size_t)n32 * 4 + 15) & ~size_t(15)));
     uint32_t* kicked = reinterpret_cast<uint32_t*>(
-        smem + (((size_t)n32 * 4 + 15) & ~size_t(15)) + (size_t)((n + 1023) / 1024 * 1024) * sizeof(GT));
+        smem + (((size_t)n32 * 4 + 15) & ~size_t(15)) +
+        (size_t)((n + 4 * BT - 1) / (4 * BT) * (4 * BT)) * sizeof(GT));
     static_assert(!STG || (F32 && sizeof(WT) == 4), "staged groups: float rows, float32 fields");
     c.stage = STG ? reinterpret_cast<WT*>(reinterpret_cast<unsigned char*>(kicked) +
                                           (((size_t)n32 * 4 + 15) & ~size_t(15)))
@@ -313,13 +317,13 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
           acc += ((c.bits[v >> 5] >> (v & 31)) & 1) ? w : -w;
         }
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
-        if (lane == 0) c.g[fpos(k)] = acc;
+        if (lane == 0) c.g[fpos<BT>(k)] = acc;
       }
     } else {
       // at most two groups per pass: eight accumulators keep the register
       // budget of three resident CTAs per SM
       constexpr int CI = CH > 2 ? 2 : CH;
-      for (int base = 4 * threadIdx.x; base < n; base += CI * 1024) {
+      for (int base = 4 * threadIdx.x; base < n; base += CI * 4 * BT) {
         GT acc[4 * CI];
 #pragma unroll
         for (int e = 0; e < 4 * CI; ++e) acc[e] = 0;
@@ -329,7 +333,7 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
           const bool xu = (c.bits[u >> 5] >> (u & 31)) & 1u;
 #pragma unroll
           for (int j = 0; j < CI; ++j) {
-            const int v = base + j * 1024;
+            const int v = base + j * 4 * BT;
             if (v < n) {
               WT w4[4];
               if (v + 3 < n) {
@@ -353,8 +357,8 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
         for (int j = 0; j < CI; ++j)
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            const int v = base + j * 1024 + i;
-            if (v < n) c.g[fpos(v)] = acc[4 * j + i];
+            const int v = base + j * 4 * BT + i;
+            if (v < n) c.g[fpos<BT>(v)] = acc[4 * j + i];
           }
       }
     }
@@ -362,7 +366,7 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
     // q = x^T W x = sum_k x_k y_k; value from q
     double part = 0.0;
     for (int v = threadIdx.x; v < n; v += blockDim.x)
-      part += ((c.bits[v >> 5] >> (v & 31)) & 1) ? (double)c.g[fpos(v)] : -(double)c.g[fpos(v)];
+      part += ((c.bits[v >> 5] >> (v & 31)) & 1) ? (double)c.g[fpos<BT>(v)] : -(double)c.g[fpos<BT>(v)];
     for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xFFFFFFFFu, part, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
     __syncthreads();
@@ -377,7 +381,7 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
     unsigned long long key;
     double gk;
     int par = 0;
-    flip_and_select<WT, GT, CH, STG>(c, -1, 0, red_key, red_g, par, &key, &gk);
+    flip_and_select<WT, GT, CH, STG, BT>(c, -1, 0, red_key, red_g, par, &key, &gk);
     par ^= 1;
     for (int r = 0; r <= rounds; ++r) {
       // steepest ascent: flip the best node while its gain is positive
@@ -389,7 +393,7 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
         }
         const int k = (int)(0x3FFFFFFFu - (((uint32_t)key) >> 1));
         val += scale * gk;  // exact gain of k before the flip
-        flip_and_select<WT, GT, CH, STG>(c, k, (int)(key & 1ull), red_key, red_g, par, &key, &gk);
+        flip_and_select<WT, GT, CH, STG, BT>(c, k, (int)(key & 1ull), red_key, red_g, par, &key, &gk);
         par ^= 1;
         ++nflips;
       }
@@ -412,11 +416,11 @@ __global__ void __launch_bounds__(256, F32 ? 4 : 3) batch_search_kernel(
           if (!((kicked[pick >> 5] >> (pick & 31)) & 1u)) break;
         }
         const int xp = (c.bits[pick >> 5] >> (pick & 31)) & 1;
-        const double gp = xp ? (double)c.g[fpos(pick)] : -(double)c.g[fpos(pick)];
+        const double gp = xp ? (double)c.g[fpos<BT>(pick)] : -(double)c.g[fpos<BT>(pick)];
         __syncthreads();  // everyone has read bit, field and kicked set before they change
         if (threadIdx.x == 0) kicked[pick >> 5] |= 1u << (pick & 31);
         val += scale * gp;
-        flip_and_select<WT, GT, CH, STG>(c, pick, xp, red_key, red_g, par, &key, &gk);
+        flip_and_select<WT, GT, CH, STG, BT>(c, pick, xp, red_key, red_g, par, &key, &gk);
         par ^= 1;
         ++nflips;
       }
@@ -652,7 +656,8 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
                                     int flip_budget, uint64_t seed, const double* kick_cdf,
                                     const long long* cdf_offset, uint32_t* best_states,
                                     double* best_values, unsigned long long* flips_total,
-                                    int* status, void* stream, bool f32) {
+                                    int* status, void* stream, bool f32, int bt) {
+  PQI_CHECK_ARG(bt == 256 || bt == 128);
   PQI_CHECK_ARG(graphs && num_graphs > 0 && task_graph && init_states && tasks > 0 && max_n > 0);
   PQI_CHECK_ARG(best_states && best_values && flips_total && status && rounds >= 0 && kick >= 0);
   PQI_CHECK_ARG(words_pitch >= (max_n + 31) / 32 && flip_budget > 0);
@@ -660,15 +665,16 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   cudaStream_t s = as_stream(stream);
   const bool i8 = kind == PQI_W_I8;
   const size_t smem = (((size_t)((max_n + 31) >> 5) * 4 + 15) & ~size_t(15)) +
-                      (size_t)((max_n + 1023) / 1024 * 1024) *
+                      (size_t)((max_n + 4 * bt - 1) / (4 * bt) * (4 * bt)) *
                           (i8 ? sizeof(int) : (f32 ? sizeof(float) : sizeof(double))) +
                       (((size_t)((max_n + 31) >> 5) * 4 + 15) & ~size_t(15));  // kicked set of the round
-  const int groups = (max_n + 1023) / 1024;  // groups of four per thread
+  const int groups = (max_n + 4 * bt - 1) / (4 * bt);  // groups of four per thread
   // float32 fields beyond four groups: four more groups per pass staged in
   // shared memory (16 KB), all of SK n = 8192's row in flight per flip
   // (staging is skipped where its buffer would not fit: every row group in registers)
   const size_t stage_bytes = (size_t)kStageGroups * 256 * 4 * sizeof(float);
-  const bool staged = f32 && !i8 && groups > 4 && !g_batch_no_stage && smem + stage_bytes <= 200 * 1024;
+  const bool staged =
+      bt == 256 && f32 && !i8 && groups > 4 && !g_batch_no_stage && smem + stage_bytes <= 200 * 1024;
   const size_t smem_all = smem + (staged ? stage_bytes : 0);
   PQI_CHECK_ARG(smem_all <= 200 * 1024);
   static int num_sms = 0;
@@ -684,39 +690,59 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   // (the whole row for n <= 4 * 256 * CH). CH = 4 keeps three CTAs per SM
   // within the register file (8 groups spill at that occupancy and run slower
   // on SK n = 8192 than two chunks of 4).
-#define PQI_BATCH_LAUNCH(WT_, CH_, F_, S_)                                                      \
+#define PQI_BATCH_LAUNCH(WT_, CH_, F_, S_, BT_)                                                 \
   do {                                                                                         \
-    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_, S_>,                        \
+    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_, S_, BT_>,                   \
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_all)); \
-    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_, S_>,                        \
+    PQI_TRY(cudaFuncSetAttribute(batch_search_kernel<WT_, CH_, F_, S_, BT_>,                   \
                                  cudaFuncAttributePreferredSharedMemoryCarveout, 100));        \
     PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                     \
-        &per_sm, batch_search_kernel<WT_, CH_, F_, S_>, 256, smem_all));                       \
+        &per_sm, batch_search_kernel<WT_, CH_, F_, S_, BT_>, BT_, smem_all));                  \
     const int grid = std::max(1, std::min(tasks, num_sms * std::max(1, per_sm)));             \
-    batch_search_kernel<WT_, CH_, F_, S_><<<grid, 256, smem_all, s>>>(                         \
+    batch_search_kernel<WT_, CH_, F_, S_, BT_><<<grid, BT_, smem_all, s>>>(                    \
         gd, task_graph, init_states, words_pitch, tasks, is_spin_glass, rounds, kick,          \
         flip_budget, seed, kick_cdf, cdf_offset, best_states, best_values, flips_total,        \
         status);                                                                               \
   } while (0)
-  if (i8) {
-    if (groups <= 2) {
-      PQI_BATCH_LAUNCH(int8_t, 2, false, false);
+  if (bt == 128) {  // small graphs: two groups per thread cover n <= 1024
+    if (i8) {
+      if (groups <= 2) {
+        PQI_BATCH_LAUNCH(int8_t, 2, false, false, 128);
+      } else {
+        PQI_BATCH_LAUNCH(int8_t, 4, false, false, 128);
+      }
+    } else if (f32) {
+      if (groups <= 2) {
+        PQI_BATCH_LAUNCH(float, 2, true, false, 128);
+      } else {
+        PQI_BATCH_LAUNCH(float, 4, true, false, 128);
+      }
     } else {
-      PQI_BATCH_LAUNCH(int8_t, 4, false, false);
+      if (groups <= 2) {
+        PQI_BATCH_LAUNCH(float, 2, false, false, 128);
+      } else {
+        PQI_BATCH_LAUNCH(float, 4, false, false, 128);
+      }
+    }
+  } else if (i8) {
+    if (groups <= 2) {
+      PQI_BATCH_LAUNCH(int8_t, 2, false, false, 256);
+    } else {
+      PQI_BATCH_LAUNCH(int8_t, 4, false, false, 256);
     }
   } else if (f32) {
     if (groups <= 2) {
-      PQI_BATCH_LAUNCH(float, 2, true, false);
+      PQI_BATCH_LAUNCH(float, 2, true, false, 256);
     } else if (staged) {
-      PQI_BATCH_LAUNCH(float, 4, true, true);
+      PQI_BATCH_LAUNCH(float, 4, true, true, 256);
     } else {
-      PQI_BATCH_LAUNCH(float, 4, true, false);
+      PQI_BATCH_LAUNCH(float, 4, true, false, 256);
     }
   } else {
     if (groups <= 2) {
-      PQI_BATCH_LAUNCH(float, 2, false, false);
+      PQI_BATCH_LAUNCH(float, 2, false, false, 256);
     } else {
-      PQI_BATCH_LAUNCH(float, 4, false, false);
+      PQI_BATCH_LAUNCH(float, 4, false, false, 256);
     }
   }
 #undef PQI_BATCH_LAUNCH
@@ -740,7 +766,7 @@ pqi_status pqi_batch_search(const void* graphs, int num_graphs, const int* task_
   return batch_search_impl(graphs, num_graphs, task_graph, init_states, words_pitch, tasks, max_n,
                            kind, is_spin_glass, rounds, kick, flip_budget, seed, kick_cdf,
                            cdf_offset, best_states, best_values, flips_total, status, stream,
-                           false);
+                           false, 256);
 }
 
 pqi_status pqi_batch_search_f32(const void* graphs, int num_graphs, const int* task_graph,
@@ -753,7 +779,21 @@ pqi_status pqi_batch_search_f32(const void* graphs, int num_graphs, const int* t
   return batch_search_impl(graphs, num_graphs, task_graph, init_states, words_pitch, tasks, max_n,
                            kind, is_spin_glass, rounds, kick, flip_budget, seed, kick_cdf,
                            cdf_offset, best_states, best_values, flips_total, status, stream,
-                           true);
+                           true, 256);
+}
+
+pqi_status pqi_batch_search_cta(const void* graphs, int num_graphs, const int* task_graph,
+                                const uint32_t* init_states, int words_pitch, int tasks,
+                                int max_n, int kind, int is_spin_glass, int rounds, int kick,
+                                int flip_budget, uint64_t seed, const double* kick_cdf,
+                                const long long* cdf_offset, uint32_t* best_states,
+                                double* best_values, unsigned long long* flips_total,
+                                int* status, int threads_per_task, int float32_fields,
+                                void* stream) {
+  return batch_search_impl(graphs, num_graphs, task_graph, init_states, words_pitch, tasks, max_n,
+                           kind, is_spin_glass, rounds, kick, flip_budget, seed, kick_cdf,
+                           cdf_offset, best_states, best_values, flips_total, status, stream,
+                           float32_fields != 0, threads_per_task);
 }
 
 pqi_status pqi_batch_search_warp(const void* graphs, int num_graphs, const int* task_graph,

@@ -275,3 +275,23 @@ def test_float32_fields_staged_rows_match_register_rows():
         x = np.where(bits, 1.0, -1.0)
         assert float(vb[t]) == pytest.approx(-0.5 * x @ W @ x, rel=1e-5)
         assert np.all(x * (W @ x) <= 1e-5 * np.abs(W).sum(axis=1).max())
+
+
+@pytest.mark.parametrize("kind", ["int", "float"])
+def test_cta128_form_matches_cta_form(kind):
+    """The 128-thread CTA form (pqi_batch_search_cta) follows the 256-thread
+    form exactly: same fields summed in the same order, same selection and
+    kick stream, so the same states, values and flip counts, for float64 and
+    float32 fields."""
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    Ws = _graphs(kind, [64, 130, 257, 700, 1000, 2500], seed=12)
+    bs = BatchedSearch([DeviceGraph(W) for W in Ws])
+    task_graph = [0, 1, 2, 3, 4, 5, 4, 3, 1]
+    words = bs.random_states(task_graph, seed=8)
+    for fields in ("f64", "f32"):
+        a = bs.run(task_graph, words, True, rounds=2, kick=5, seed=4, fields=fields)
+        b = bs.run(task_graph, words, True, rounds=2, kick=5, seed=4, fields=fields, variant="cta128")
+        assert int(a[3].item()) == 0 and int(b[3].item()) == 0
+        assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) and int(a[2].item()) == int(b[2].item())
