@@ -332,10 +332,10 @@ pqi_status pqi_batch_search_f32(const void* graphs, int num_graphs, const int* t
                                 int* status, void* stream);
 
 /* pqi_batch_search (float32_fields 0) or pqi_batch_search_f32 (1) with the
- * CTA size given: threads_per_task 256 (those entry points' size) or 128 (twice
- * the resident tasks per SM at the same registers per thread; for graphs of up
- * to about a thousand nodes). Same results for either size. No reference
- * counterpart (batched form of spin_glass_solver.py:603-717). */
+ * CTA size given: threads_per_task 256 (those entry points' size), 128 or 64
+ * (two or four times the resident tasks per SM at the same registers per
+ * thread; for graphs of up to a few thousand nodes). Same results for every
+ * size. No reference counterpart (batched form of spin_glass_solver.py:603-717). */
 pqi_status pqi_batch_search_cta(const void* graphs, int num_graphs, const int* task_graph,
                                 const uint32_t* init_states, int words_pitch, int tasks,
                                 int max_n, int kind, int is_spin_glass, int rounds, int kick,

@@ -78,9 +78,9 @@ class BatchedSearch:
             flip_budget: int | None = None, variant: str = "cta", warps_per_sm: int = 0, out=None,
             fields: str = "f64"):
         """Iterated local search of every task. variant: "cta" (one CTA of 256
-        threads per task, any n), "cta128" (one CTA of 128 threads: twice the
-        resident tasks, for small graphs) or "warp" (one warp per task, max_n
-        <= 1024); all give the same results. fields: "f64" (default) or "f32" (CTA form, float
+        threads per task, any n), "cta128" / "cta64" (CTAs of 128 / 64 threads:
+        two / four times the resident tasks, for small graphs) or "warp" (one
+        warp per task, max_n <= 1024); all give the same results. fields: "f64" (default) or "f32" (CTA form, float
         graphs: float32 local fields, more resident tasks per SM; rounding can
         change trajectories). `out` = (best_states, best_values, flips, status)
         device buffers to fill (for CUDA-graph capture); flips and status are
@@ -104,16 +104,16 @@ class BatchedSearch:
                 D.stream_ptr(self.stream),
             )
             return best_values, best_states.view(tasks, self.pitch), flips, status
-        if variant not in ("cta", "cta128"):
-            raise ValueError("variant must be 'cta', 'cta128' or 'warp'")
+        if variant not in ("cta", "cta128", "cta64"):
+            raise ValueError("variant must be 'cta', 'cta128', 'cta64' or 'warp'")
         if fields not in ("f64", "f32"):
             raise ValueError("fields must be 'f64' or 'f32'")
-        if variant == "cta128":
+        if variant in ("cta128", "cta64"):
             _lib.call(
                 "pqi_batch_search_cta", D._ptr(self.desc), len(self.graphs), D._ptr(tg), D._ptr(init_words),
                 self.pitch, tasks, self.max_n, int(self.kind), int(bool(is_spin_glass)), int(rounds), int(kick),
                 budget, ctypes.c_uint64(int(seed) & 0xFFFFFFFFFFFFFFFF), D._ptr(kick_cdf), D._ptr(cdf_offset),
-                D._ptr(best_states), D._ptr(best_values), D._ptr(flips), D._ptr(status), 128,
+                D._ptr(best_states), D._ptr(best_values), D._ptr(flips), D._ptr(status), int(variant[3:]),
                 int(fields == "f32"), D.stream_ptr(self.stream),
             )
             return best_values, best_states.view(tasks, self.pitch), flips, status
@@ -194,7 +194,7 @@ class BatchedSolver:
     per graph over its seeds (reduced on the device).
     """
 
-    FORMS = (("cta", 0), ("cta128", 0), ("warp", 0), ("warp", 16), ("warp", 8))
+    FORMS = (("cta", 0), ("cta128", 0), ("cta64", 0), ("warp", 0), ("warp", 16), ("warp", 8))
 
     def __init__(self, graphs: list[D.DeviceGraph], seeds_per_graph: int, is_spin_glass: bool,
                  rounds: int = 0, kick: int = 8, seed: int = 0, stream=None):
@@ -233,7 +233,7 @@ class BatchedSolver:
             words = bs.random_states(tg.cpu().numpy(), seed=self.seed + 99)
             times = {}
             for form, wps in self.FORMS:
-                if (form == "warp" and bs.max_n > 1024) or (form == "cta128" and bs.max_n > 2048):
+                if (form == "warp" and bs.max_n > 1024) or (form in ("cta128", "cta64") and bs.max_n > 2048):
                     continue
                 best = float("inf")
                 for _ in range(reps + 1):  # first run warms the launch

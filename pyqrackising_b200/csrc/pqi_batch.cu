@@ -266,8 +266,8 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
 // STG (float32 fields only): each flip pass also stages kStageGroups row
 // groups per thread through cp.async, so a pass of SK n = 8192 has its whole
 // 32 KB row in flight at once instead of in two register chunks.
-// BT: threads per CTA (256; 128 for small graphs: twice the resident tasks per
-// SM, at the same registers per thread).
+// BT: threads per CTA (256; 128 or 64 for small graphs: two or four times the
+// resident tasks per SM, at the same registers per thread).
 template <typename WT, int CH, bool F32, bool STG, int BT>
 __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_kernel(
     const BatchGraph* __restrict__ graphs, const int* __restrict__ task_graph,
@@ -657,7 +657,7 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
                                     const long long* cdf_offset, uint32_t* best_states,
                                     double* best_values, unsigned long long* flips_total,
                                     int* status, void* stream, bool f32, int bt) {
-  PQI_CHECK_ARG(bt == 256 || bt == 128);
+  PQI_CHECK_ARG(bt == 256 || bt == 128 || bt == 64);
   PQI_CHECK_ARG(graphs && num_graphs > 0 && task_graph && init_states && tasks > 0 && max_n > 0);
   PQI_CHECK_ARG(best_states && best_values && flips_total && status && rounds >= 0 && kick >= 0);
   PQI_CHECK_ARG(words_pitch >= (max_n + 31) / 32 && flip_budget > 0);
@@ -704,7 +704,27 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
         flip_budget, seed, kick_cdf, cdf_offset, best_states, best_values, flips_total,        \
         status);                                                                               \
   } while (0)
-  if (bt == 128) {  // small graphs: two groups per thread cover n <= 1024
+  if (bt == 64) {  // smallest graphs: four groups per thread cover n <= 1024
+    if (i8) {
+      if (groups <= 2) {
+        PQI_BATCH_LAUNCH(int8_t, 2, false, false, 64);
+      } else {
+        PQI_BATCH_LAUNCH(int8_t, 4, false, false, 64);
+      }
+    } else if (f32) {
+      if (groups <= 2) {
+        PQI_BATCH_LAUNCH(float, 2, true, false, 64);
+      } else {
+        PQI_BATCH_LAUNCH(float, 4, true, false, 64);
+      }
+    } else {
+      if (groups <= 2) {
+        PQI_BATCH_LAUNCH(float, 2, false, false, 64);
+      } else {
+        PQI_BATCH_LAUNCH(float, 4, false, false, 64);
+      }
+    }
+  } else if (bt == 128) {  // small graphs: two groups per thread cover n <= 1024
     if (i8) {
       if (groups <= 2) {
         PQI_BATCH_LAUNCH(int8_t, 2, false, false, 128);

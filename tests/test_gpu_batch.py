@@ -292,6 +292,7 @@ def test_cta128_form_matches_cta_form(kind):
     words = bs.random_states(task_graph, seed=8)
     for fields in ("f64", "f32"):
         a = bs.run(task_graph, words, True, rounds=2, kick=5, seed=4, fields=fields)
-        b = bs.run(task_graph, words, True, rounds=2, kick=5, seed=4, fields=fields, variant="cta128")
-        assert int(a[3].item()) == 0 and int(b[3].item()) == 0
-        assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) and int(a[2].item()) == int(b[2].item())
+        for variant in ("cta128", "cta64"):
+            b = bs.run(task_graph, words, True, rounds=2, kick=5, seed=4, fields=fields, variant=variant)
+            assert int(a[3].item()) == 0 and int(b[3].item()) == 0
+            assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) and int(a[2].item()) == int(b[2].item())
