@@ -187,9 +187,9 @@ class BatchedSolver:
     """Many graphs of mixed weight kinds, many starting states per graph.
 
     Graphs are grouped by weight kind (int8 vs float32 launches). For each
-    group a small autotuner times the kernel forms (one CTA per task, or one
-    warp per task with an occupancy cap) on a sample of tasks and keeps the
-    fastest; `capture()` then records every launch of a step in one CUDA
+    group a small autotuner times the kernel forms (one CTA of 256, 128 or 64
+    threads per task, or one warp per task with an occupancy cap) on the
+    group's tasks and keeps the fastest; `capture()` then records every launch of a step in one CUDA
     graph, so a step is one graph replay. Results are the best value and state
     per graph over its seeds (reduced on the device).
     """
