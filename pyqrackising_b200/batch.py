@@ -17,14 +17,18 @@ import torch
 
 from . import _lib
 from . import device as D
+from .maxcut_tfim import row_lists as _row_lists  # (kept on each DeviceGraph, alive with it)
 
-_DESC = np.dtype([("W", "<u8"), ("n", "<i4"), ("ld", "<i4"), ("kind", "<i4"), ("pad", "<i4"), ("upper_sum", "<f8")])
+_DESC = np.dtype([("W", "<u8"), ("n", "<i4"), ("ld", "<i4"), ("kind", "<i4"), ("pad", "<i4"), ("upper_sum", "<f8"),
+                  ("adj_ptr", "<u8"), ("adj_col", "<u8"), ("adj_val", "<u8")])
 
 
 class BatchedSearch:
     """Iterated local search over a set of prepared graphs sharing one weight kind."""
 
-    def __init__(self, graphs: list[D.DeviceGraph], stream=None):
+    def __init__(self, graphs: list[D.DeviceGraph], stream=None, row_lists: bool = True):
+        """row_lists: give sparse graphs (at most a quarter of W nonzero) their
+        row lists, so the CTA form's starting fields cost O(nonzeros)."""
         if not graphs:
             raise ValueError("no graphs")
         kinds = {g.w.kind for g in graphs}
@@ -44,6 +48,11 @@ class BatchedSearch:
             desc[i]["ld"] = g.ld
             desc[i]["kind"] = g.w.kind
             desc[i]["upper_sum"] = g.upper_sum
+            rl = _row_lists(g) if row_lists else None
+            if rl is not None:
+                desc[i]["adj_ptr"] = rl[0].data_ptr()
+                desc[i]["adj_col"] = rl[1].data_ptr()
+                desc[i]["adj_val"] = rl[2].data_ptr()
         self.desc = torch.from_numpy(desc.view(np.uint8).copy()).to(self.device)
         self.n = np.array([g.n for g in graphs], dtype=np.int64)
 

@@ -32,6 +32,13 @@ struct BatchGraph {
   int kind;
   int pad;
   double upper_sum;
+  // optional row lists of the graph's nonzero weights (row r: columns
+  // adj_col[adj_ptr[r] .. adj_ptr[r+1]) ascending, values adj_val; the
+  // diagonal may be listed and is skipped): the starting fields then cost
+  // O(nonzeros) instead of O(n^2)
+  const long long* adj_ptr;
+  const int* adj_col;
+  const float* adj_val;
 };
 
 __device__ __forceinline__ uint64_t bmix64(uint64_t z) {
@@ -302,12 +309,26 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
     for (int w = threadIdx.x; w < n32; w += blockDim.x) c.bits[w] = init_states[(size_t)task * words_pitch + w];
     __syncthreads();
     // 1. local fields of the starting state, y_v = sum_u x_u W_uv (W is
-    // symmetric). Below 2048 nodes a warp per row (row dot product, shuffle
-    // reduction): more rows in flight per CTA. From 2048 nodes every row u adds
+    // symmetric). With row lists, each field sums its own row's nonzero
+    // entries in column order (the dense column-order sum without its zero
+    // terms). Else, below 2048 nodes a warp per row (row dot product, shuffle
+    // reduction): more rows in flight per CTA; from 2048 nodes every row u adds
     // +-W_u to each thread's own nodes (rows ascending, CH groups of four per
     // pass in registers): a memory stream with few instructions, which leaves
     // the SM to the flips of the other resident tasks.
-    if (n < 2048) {
+    if (G.adj_ptr) {
+      for (int v = threadIdx.x; v < n; v += blockDim.x) {
+        GT acc = 0;
+        const long long e1 = G.adj_ptr[v + 1];
+        for (long long e = G.adj_ptr[v]; e < e1; ++e) {
+          const int u = G.adj_col[e];
+          if (u == v) continue;
+          const GT w = (GT)G.adj_val[e];
+          acc += ((c.bits[u >> 5] >> (u & 31)) & 1) ? w : -w;
+        }
+        c.g[fpos<BT>(v)] = acc;
+      }
+    } else if (n < 2048) {
       const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
       for (int k = threadIdx.x >> 5; k < n; k += warps) {
         const WT* row = c.W + (size_t)k * c.ld;

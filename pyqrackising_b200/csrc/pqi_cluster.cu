@@ -43,6 +43,9 @@ struct ClusterGraph {  // same layout as the batched search's graph descriptor
   int kind;
   int pad;
   double upper_sum;
+  const void* adj_ptr;  // row lists (unused here)
+  const void* adj_col;
+  const void* adj_val;
 };
 
 struct Slot {

@@ -296,3 +296,36 @@ def test_cta128_form_matches_cta_form(kind):
             b = bs.run(task_graph, words, True, rounds=2, kick=5, seed=4, fields=fields, variant=variant)
             assert int(a[3].item()) == 0 and int(b[3].item()) == 0
             assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) and int(a[2].item()) == int(b[2].item())
+
+
+def test_row_list_starts_match_dense_starts():
+    """Starting fields from row lists (sparse graphs) against the dense row
+    reads: int8 graphs give identical searches (exact sums); float graphs of
+    2048+ nodes too (both sum each field in column order); smaller float
+    graphs (the dense start reduces by warp shuffles) end at local optima with
+    values equal to float64 re-scoring."""
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    for kind, sizes, exact in (("int", [64, 300, 1000, 2100], True), ("float", [2100, 2600], True),
+                               ("float", [100, 700], False)):
+        Ws = _graphs(kind, sizes, seed=30)
+        dgs = [DeviceGraph(W) for W in Ws]
+        with_lists = BatchedSearch(dgs)
+        dense = BatchedSearch(dgs, row_lists=False)
+        task_graph = [i % len(Ws) for i in range(3 * len(Ws))]
+        words = with_lists.random_states(task_graph, seed=9)
+        for variant in ("cta", "cta64"):
+            a = with_lists.run(task_graph, words, True, rounds=1, kick=4, seed=1, variant=variant)
+            b = dense.run(task_graph, words, True, rounds=1, kick=4, seed=1, variant=variant)
+            assert int(a[3].item()) == 0 and int(b[3].item()) == 0
+            if exact:
+                assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1]) and int(a[2].item()) == int(b[2].item())
+            else:
+                for t, g in enumerate(task_graph):
+                    bits = with_lists.unpack(a[1], task_graph)[t]
+                    W = Ws[g].astype(np.float64)
+                    np.fill_diagonal(W, 0.0)
+                    x = np.where(bits, 1.0, -1.0)
+                    assert float(a[0][t]) == pytest.approx(-0.5 * x @ W @ x, rel=1e-9, abs=1e-9)
+                    assert np.all(x * (W @ x) <= 1e-9 * np.abs(W).sum(axis=1).max())
