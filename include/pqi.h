@@ -289,7 +289,10 @@ pqi_status pqi_exact_search(const float* W, int n, int is_spin_glass, double* be
 
 /* Size of one graph descriptor in the device array pqi_batch_search reads:
  * {const void* W (prepared W_i8 or W_f32z); int n; int ld; int kind; int pad;
- *  double upper_sum}. */
+ *  double upper_sum; const long long* adj_ptr; const int* adj_col;
+ *  const float* adj_val} -- the last three the row lists of a sparse graph's
+ * nonzero weights (pqi_tfim_adj_count / pqi_tfim_adj_fill; the diagonal may be
+ * listed and is skipped), used for the starting fields, or null. */
 size_t pqi_batch_graph_desc_bytes(void);
 
 /*
