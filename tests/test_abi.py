@@ -77,3 +77,16 @@ def test_no_cpu_fallback_without_library(monkeypatch, tmp_path):
     monkeypatch.setattr(_lib, "_lib", None)
     with pytest.raises(_lib.PQIUnavailable):
         _lib.load(str(tmp_path / "missing.so"))
+
+
+def test_graph_descriptor_layout_matches_the_library():
+    """The batched entry points read an array of C structs; the host packs it
+    with a numpy dtype. Size and field offsets must agree (the row-list
+    pointers follow upper_sum)."""
+    from pyqrackising_b200 import _lib
+    from pyqrackising_b200.batch import _DESC
+
+    assert _lib.load().pqi_batch_graph_desc_bytes() == _DESC.itemsize == 56
+    offsets = {name: _DESC.fields[name][1] for name in _DESC.names}
+    assert offsets == {"W": 0, "n": 8, "ld": 12, "kind": 16, "pad": 20, "upper_sum": 24,
+                       "adj_ptr": 32, "adj_col": 40, "adj_val": 48}
