@@ -82,3 +82,12 @@ def test_coordinate_list_rebuilds_the_host_expansion():
     dup = coo_matrix((np.array([1.0, 2.0, 3.0], dtype=np.float32), (np.array([0, 0, 1]), np.array([1, 1, 2]))),
                      shape=(3, 3))
     assert not sparse_coordinates(dup)[5]
+
+
+def test_hybrid_refuses_matrix_input():
+    """spin_glass_solver_hybrid takes an nx.Graph only, as the reference
+    (spin_glass_solver_hybrid.py:22-23); the check runs before any device work."""
+    from pyqrackising_b200 import spin_glass_solver_hybrid
+
+    with pytest.raises(TypeError):
+        spin_glass_solver_hybrid(np.zeros((30, 30), dtype=np.float32))
