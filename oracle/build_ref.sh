@@ -4,10 +4,11 @@
 # in place under the reference checkout) as C with the shim in ref_shim.h, and
 # links them with the ND-range emulator in ref_launch.c into
 # oracle/_ref/libpqi_ref.so. The output stays out of version control.
-# Usage: oracle/build_ref.sh [reference_root]   (default /root/reference)
+# Usage: oracle/build_ref.sh [reference_root]
+#   (default: $PQI_REFERENCE_ROOT, else the build container's /root/reference)
 set -eu
 HERE=$(cd "$(dirname "$0")" && pwd)
-REF=${1:-/root/reference}
+REF=${1:-${PQI_REFERENCE_ROOT:-/root/reference}}
 SRC="$REF/pyqrackising/kernels.cl"
 if [ ! -f "$SRC" ]; then
   echo "reference kernels not found at $SRC" >&2

@@ -47,9 +47,18 @@ def build_oracle(force: bool = False) -> str:
     return ORACLE_SO
 
 
-def build_ref(reference_root: str = "/root/reference") -> str | None:
+def reference_root() -> str:
+    """Where the reference checkout lies in the build container: the
+    environment variable PQI_REFERENCE_ROOT, else the container's read-only
+    mount. Only build recipes and fixture generators read it."""
+    return os.environ.get("PQI_REFERENCE_ROOT", "/root/reference")
+
+
+def build_ref(reference_root: str | None = None) -> str | None:
     """Build ``oracle/_ref/libpqi_ref.so`` from the reference's kernels.cl when the
     reference checkout is present; returns None otherwise."""
+    if reference_root is None:
+        reference_root = globals()["reference_root"]()
     if not os.path.exists(os.path.join(reference_root, "pyqrackising", "kernels.cl")):
         return None
     subprocess.check_call(["sh", os.path.join(HERE, "build_ref.sh"), reference_root])
@@ -57,6 +66,7 @@ def build_ref(reference_root: str = "/root/reference") -> str | None:
 
 
 _F32P = ctypes.POINTER(ctypes.c_float)
+_F64P = ctypes.POINTER(ctypes.c_double)
 _U32P = ctypes.POINTER(ctypes.c_uint32)
 _U64P = ctypes.POINTER(ctypes.c_uint64)
 _I32P = ctypes.POINTER(ctypes.c_int32)
@@ -86,6 +96,9 @@ def lib():
         L.orc_double_select.restype = ctypes.c_int
         L.orc_gray_seed.argtypes = [_U64P, ctypes.c_int, ctypes.c_long]
         L.orc_gray.argtypes = [_F32P, ctypes.c_int, _U64P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _U64P, _F32P, _I64P]
+        L.orc_gray_margin.argtypes = [_F32P, ctypes.c_int, _U64P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _U64P, _F32P, _I64P, _F32P]
+        L.orc_double_select_gains.argtypes = [_F64P, _F32P, ctypes.c_int, _U32P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _F32P, _I32P]
+        L.orc_double_select_gains.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -281,17 +294,39 @@ def gray_seed(theta64, n, gid) -> np.ndarray:
     return w
 
 
-def gray(W, theta64, is_spin_glass, iters_bound, G):
-    """Returns (theta_out uint64[G, blocks], energy_out float32[G], skipped_oob_flips)."""
+def gray(W, theta64, is_spin_glass, iters_bound, G, margins=False):
+    """Returns (theta_out uint64[G, blocks], energy_out float32[G], skipped_oob_flips)
+    and, with margins=True, a fourth item: float32[G], each work-item's smallest
+    |gain| over its keep-or-revert decisions (inf when it made none)."""
     W = _w(W)
     n = W.shape[0]
     blocks = (n + 63) >> 6
     th = np.ascontiguousarray(theta64, dtype=np.uint64)
     tout = np.empty((G, blocks), dtype=np.uint64)
     eout = np.empty(G, dtype=np.float32)
+    marg = np.empty(G, dtype=np.float32)
     oob = ctypes.c_int64()
-    lib().orc_gray(_p(W, _F32P), n, _p(th, _U64P), int(bool(is_spin_glass)), int(iters_bound), int(G), _p(tout, _U64P), _p(eout, _F32P), ctypes.byref(oob))
+    lib().orc_gray_margin(_p(W, _F32P), n, _p(th, _U64P), int(bool(is_spin_glass)), int(iters_bound), int(G),
+                          _p(tout, _U64P), _p(eout, _F32P), ctypes.byref(oob), _p(marg, _F32P))
+    if margins:
+        return tout, eout, int(oob.value), marg
     return tout, eout, int(oob.value)
+
+
+def double_select_gains(W, theta32, gains64, is_spin_glass, G, L):
+    """The double-flip pass's selection (kernels.cl:186-231) with pair values
+    from float64 gains, each rounded once to float32 (pqi_oracle.c
+    orc_double_select_gains): the reference's exact result for integer
+    weights, O(n^2) so it runs at full benchmark sizes."""
+    W = _w(W)
+    th = np.ascontiguousarray(theta32, dtype=np.uint32)
+    g = np.ascontiguousarray(gains64, dtype=np.float64)
+    e = ctypes.c_float()
+    i = ctypes.c_int32()
+    if lib().orc_double_select_gains(_p(g, _F64P), _p(W, _F32P), W.shape[0], _p(th, _U32P), int(bool(is_spin_glass)),
+                                     int(G), int(L), ctypes.byref(e), ctypes.byref(i)) != 0:
+        raise ValueError("bad geometry")
+    return np.float32(e.value), int(i.value)
 
 
 def gray_has_oob(n, iters_bound, G) -> bool:

@@ -74,6 +74,8 @@ float orc_single_one(const float* W, int n, const uint32_t* th, int k) {
 
 /* Per-item values of single_bit_flips (kernels.cl:118-148), x2 for spin glass. */
 void orc_single_values(const float* W, int n, const uint32_t* th, int is_spin_glass, float* out) {
+  /* items are independent: threads do not change any value */
+#pragma omp parallel for schedule(static)
   for (int k = 0; k < n; ++k) {
     float e = orc_single_one(W, n, th, k);
     if (is_spin_glass) e *= 2.0f;
@@ -219,16 +221,24 @@ void orc_gray_seed(uint64_t* words, int n, long gid) {
 
 /* Gray-code walk of the gray kernel (kernels.cl:894-978) for all G work-items.
  * iters_bound is args[2] = ceil(gray_iterations / G). theta_out is G*blocks
- * words, energy_out is G floats. *oob counts flips skipped because k >= n. */
-void orc_gray(const float* W, int n, const uint64_t* theta, int is_spin_glass, int iters_bound,
-              int G, uint64_t* theta_out, float* energy_out, long* oob) {
+ * words, energy_out is G floats. *oob counts flips skipped because k >= n.
+ * margin_out (G floats, may be NULL) receives, per work-item, the smallest
+ * |gain| over all of its keep-or-revert decisions (+inf if it made none): a
+ * walk whose every decision clears a rounding bound is decided the same way
+ * by any evaluation of the gains within that bound. Work-items are
+ * independent, so they run on OpenMP threads without changing any value. */
+void orc_gray_margin(const float* W, int n, const uint64_t* theta, int is_spin_glass,
+                     int iters_bound, int G, uint64_t* theta_out, float* energy_out, long* oob,
+                     float* margin_out) {
   const int blocks = (n + 63) >> 6;
-  uint64_t* loc = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)blocks);
   long skipped = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : skipped)
   for (int gid = 0; gid < G; ++gid) {
+    uint64_t* loc = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)blocks);
     memcpy(loc, theta, sizeof(uint64_t) * (size_t)blocks);
     orc_gray_seed(loc, n, gid);
     float e = 0.0f;
+    float margin = INFINITY;
     for (int u = 0; u < n; ++u) {
       const float* row = W + (size_t)u * n;
       const int ou = bit64(theta, u), nu = bit64(loc, u);
@@ -255,6 +265,7 @@ void orc_gray(const float* W, int n, const uint64_t* theta, int is_spin_glass, i
           const float w = row[v];
           g += (kb == bit64(loc, v)) ? -w : w;
         }
+        if (fabsf(g) < margin) margin = fabsf(g);
         if (g > 0.0f) {
           e += g;
         } else {
@@ -265,7 +276,53 @@ void orc_gray(const float* W, int n, const uint64_t* theta, int is_spin_glass, i
     memcpy(theta_out + (size_t)gid * blocks, loc, sizeof(uint64_t) * (size_t)blocks);
     if (!is_spin_glass) e /= 2;
     energy_out[gid] = e;
+    if (margin_out) margin_out[gid] = margin;
+    free(loc);
   }
-  free(loc);
   if (oob) *oob = skipped;
+}
+
+void orc_gray(const float* W, int n, const uint64_t* theta, int is_spin_glass, int iters_bound,
+              int G, uint64_t* theta_out, float* energy_out, long* oob) {
+  orc_gray_margin(W, n, theta, is_spin_glass, iters_bound, G, theta_out, energy_out, oob, NULL);
+}
+
+/* double_bit_flips selection (kernels.cl:186-231) with each pair value taken
+ * from float64 single-flip gains: value(k, l) = g_k + g_l - 2 s_kl W_kl with
+ * s_kl = +1 when bits k and l agree, else -1 (doubled for a spin glass),
+ * rounded once to float32. For integer weights whose partial sums stay below
+ * 2^24 this is exactly the reference's float32 sum over v, so the selected
+ * (value, pair) is the reference's; it costs O(n^2) instead of O(n^3), which
+ * makes full-size instances checkable. Pairs are visited in the reference's
+ * k-major linear order and dealt to work-items by index modulo G. */
+int orc_double_select_gains(const double* gains, const float* W, int n, const uint32_t* th,
+                            int is_spin_glass, int G, int L, float* best_e, int* best_i) {
+  if (G <= 0 || L <= 0 || G % L) return -1;
+  float* te = (float*)malloc(sizeof(float) * (size_t)G);
+  int* ti = (int*)malloc(sizeof(int) * (size_t)G);
+  for (int t = 0; t < G; ++t) {
+    te[t] = -INFINITY;
+    ti[t] = t;
+  }
+  long c = 0;
+  int t = 0;
+  for (int k = 0; k < n; ++k) {
+    const float* row = W + (size_t)k * n;
+    const int kb = bit32(th, k);
+    for (int l = k + 1; l < n; ++l, ++c) {
+      const double sgn = (kb == bit32(th, l)) ? 1.0 : -1.0;
+      double v = gains[k] + gains[l] - 2.0 * sgn * (double)row[l];
+      if (is_spin_glass) v *= 2.0;
+      const float e = (float)v;
+      if (e > te[t]) {
+        te[t] = e;
+        ti[t] = (int)c;
+      }
+      if (++t == G) t = 0;
+    }
+  }
+  fold_threads(te, ti, G, L, best_e, best_i, NULL, NULL);
+  free(te);
+  free(ti);
+  return 0;
 }

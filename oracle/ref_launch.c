@@ -8,8 +8,9 @@
  * Each work-group runs as L POSIX threads (L = local size, <= 32 on the
  * reference's launch shapes, maxcut_tfim_util.py:169-221) that share one
  * pthread barrier, so reduce_energy_index (kernels.cl:1-29) executes with its
- * real barrier semantics. Work-groups run one after another, which is a legal
- * OpenCL schedule because the kernels do not communicate across groups.
+ * real barrier semantics. Work-groups run concurrently, in waves of up to 256
+ * work-items (every group with its own barrier and local arrays), which is a
+ * legal OpenCL schedule because the kernels do not communicate across groups.
  *
  * The launch arguments mirror the host glue of the reference:
  *   calculate_cut     args = [n, shots, is_spin_glass, seg, theta_seg]  (maxcut_tfim.py:167-171)
@@ -92,48 +93,54 @@ static int launch_reducing(int kind, const float* W, const void* theta, const in
                            int L, float* max_e, int* max_i) {
   if (G <= 0 || L <= 0 || L > 1024 || G % L) return -1;
   const int groups = G / L;
-  work_item* items = (work_item*)calloc((size_t)L, sizeof(work_item));
-  pthread_t* th = (pthread_t*)calloc((size_t)L, sizeof(pthread_t));
-  float* loc_e = (float*)calloc((size_t)L, sizeof(float));
-  int* loc_i = (int*)calloc((size_t)L, sizeof(int));
-  if (!items || !th || !loc_e || !loc_i) return -2;
+  const int wave = L >= 256 ? 1 : 256 / L;  /* groups running at once */
+  work_item* items = (work_item*)calloc((size_t)wave * L, sizeof(work_item));
+  pthread_t* th = (pthread_t*)calloc((size_t)wave * L, sizeof(pthread_t));
+  float* loc_e = (float*)calloc((size_t)wave * L, sizeof(float));
+  int* loc_i = (int*)calloc((size_t)wave * L, sizeof(int));
+  pthread_barrier_t* bars = (pthread_barrier_t*)calloc((size_t)wave, sizeof(pthread_barrier_t));
+  if (!items || !th || !loc_e || !loc_i || !bars) return -2;
   pthread_attr_t attr;
   pthread_attr_init(&attr);
   pthread_attr_setstacksize(&attr, 1 << 20);
-  for (int g = 0; g < groups; ++g) {
-    pthread_barrier_t bar;
-    pthread_barrier_init(&bar, NULL, (unsigned)L);
-    for (int l = 0; l < L; ++l) {
-      work_item* it = &items[l];
-      it->kind = kind;
-      it->W = W;
-      it->theta = theta;
-      it->args = args;
-      it->max_e = max_e;
-      it->max_i = max_i;
-      it->loc_e = loc_e;
-      it->loc_i = loc_i;
-      it->gid = (size_t)g * L + l;
-      it->lid = (size_t)l;
-      it->grp = (size_t)g;
-      it->gsize = (size_t)G;
-      it->lsize = (size_t)L;
-      it->bar = &bar;
-      if (L == 1) {
-        run_item(it);
-      } else {
-        pthread_create(&th[l], &attr, run_item, it);
+  for (int g0 = 0; g0 < groups; g0 += wave) {
+    const int gn = groups - g0 < wave ? groups - g0 : wave;
+    for (int q = 0; q < gn; ++q) pthread_barrier_init(&bars[q], NULL, (unsigned)L);
+    for (int q = 0; q < gn; ++q) {
+      const int g = g0 + q;
+      for (int l = 0; l < L; ++l) {
+        work_item* it = &items[(size_t)q * L + l];
+        it->kind = kind;
+        it->W = W;
+        it->theta = theta;
+        it->args = args;
+        it->max_e = max_e;
+        it->max_i = max_i;
+        it->loc_e = loc_e + (size_t)q * L;
+        it->loc_i = loc_i + (size_t)q * L;
+        it->gid = (size_t)g * L + l;
+        it->lid = (size_t)l;
+        it->grp = (size_t)g;
+        it->gsize = (size_t)G;
+        it->lsize = (size_t)L;
+        it->bar = &bars[q];
+        if (L == 1 && gn == 1) {
+          run_item(it);
+        } else {
+          pthread_create(&th[(size_t)q * L + l], &attr, run_item, it);
+        }
       }
     }
-    if (L > 1)
-      for (int l = 0; l < L; ++l) pthread_join(th[l], NULL);
-    pthread_barrier_destroy(&bar);
+    if (L > 1 || gn > 1)
+      for (int t = 0; t < gn * L; ++t) pthread_join(th[t], NULL);
+    for (int q = 0; q < gn; ++q) pthread_barrier_destroy(&bars[q]);
   }
   pthread_attr_destroy(&attr);
   free(items);
   free(th);
   free(loc_e);
   free(loc_i);
+  free(bars);
   return 0;
 }
 

@@ -53,14 +53,21 @@ def build(force: bool = False, verbose: bool = False, extra=None) -> str:
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [nvcc(), *NVCC_FLAGS, *(extra or []), "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
+        cmds.append([nvcc(), *NVCC_FLAGS, *(extra or []), "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj])
+        objs.append(obj)
+    # one nvcc per translation unit, a few at a time
+    from concurrent.futures import ThreadPoolExecutor
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.check_call(cmd)
-        objs.append(obj)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as pool:
+        list(pool.map(run, cmds))
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *NVCC_FLAGS, "-shared", *objs, "-o", tmp]
     if verbose:
