@@ -17,8 +17,12 @@ and selected with its tie rule. One step = one batch.
   through the C ABI and reads the (best value, index) pair back.
 * roofline: the scoring GEMM (2*B*n^2 integer ops per launch) against the
   int8 tensor rate, taken as twice the measured dense bf16 rate.
-* cpu_baseline: the reference's calculate_cut compiled for the host (or the
-  oracle's C port of it) on the host cores, over a bounded sample of the batch.
+* cpu_baseline: the reference's CPU scoring path (numba: compute_cut_diff_between
+  per candidate under prange, maxcut_tfim.py:77-136), restated in
+  oracle/numba_port.py and pinned to the reference's own values, on all host
+  threads over a bounded sample of the batch; beside it the reference's
+  OpenCL calculate_cut compiled for the host (oracle/_ref).
+* --impl reference: the same CPU scoring as the reference arm, same config.
 * time_to_best: the other half of the metric, on the Sherrington-Kirkpatrick
   spin glass (n = 8192, J ~ N(0,1)/sqrt(n) float32): wall time of the plain
   GPU form (spin_glass_solver's local-search loop from one start) against the
@@ -143,16 +147,16 @@ class ClockSampler:
         }
 
 
-def _ref_or_port():
+def _emulator_or_c_port():
     """The reference's own kernels.cl built for the host (oracle/_ref) when it was
-    built in this checkout, else the oracle's C port."""
+    built in this checkout, else the oracle's C port of it."""
     from oracle import oracle as O
 
     O.build_oracle()
     return O, ("reference" if O.ref_available() else "port")
 
 
-def _score_sample(O, kind, W, th, sample):
+def _kernels_cl_sample(O, kind, W, th, sample):
     G, L = O.cut_geometry(sample, 148)
     if kind == "reference":
         # calculate_cut as the reference launches it: G work-items in groups of L
@@ -163,50 +167,94 @@ def _score_sample(O, kind, W, th, sample):
     return e, i
 
 
-def cpu_baseline(W, X, sample=256, max_seconds=20.0):
-    """The reference's scoring on the host cores over a bounded sample."""
-    O, kind = _ref_or_port()
-    th = O.pack32(X[:sample])
-    _score_sample(O, kind, W, th[:32], 32)  # warm
-    done = 0
+class NumbaScoring:
+    """The reference's CPU candidate scoring (numba, maxcut_tfim.py:77-136 with
+    compute_cut_diff_between, maxcut_tfim_util.py:445-461) as the oracle restates
+    it (oracle/numba_port.py), on all the host threads numba uses; the C port of
+    calculate_cut (OpenMP) when numba is absent."""
+
+    def __init__(self, W):
+        from oracle import numba_port as P
+
+        self.W = W
+        self.numba = P.available()
+        if self.numba:
+            P.warm()
+            self.P = P
+            self.cores = P.threads()
+            self.kind_text = ("the reference's CPU scoring (numba prange over candidates, compute_cut_diff_between "
+                              "against the all-false start, first max) restated in oracle/numba_port.py")
+        else:
+            from oracle import oracle as O
+
+            O.build_oracle()
+            self.O = O
+            self.cores = os.cpu_count() or 1
+            self.kind_text = "the oracle's C port of calculate_cut (OpenMP over candidates); numba is not installed"
+
+    def __call__(self, X):
+        if self.numba:
+            return self.P.select_first_max(self.P.score_batch(X, self.W))
+        v = self.O.cut_values(self.W, self.O.pack32(X), X.shape[0], 0)
+        i = int(np.argmax(v))
+        return float(v[i]), i
+
+
+def cpu_baseline(W, X, sample=2048):
+    """The reference's CPU scoring on the host cores over a bounded sample of the
+    batch (about 10-20 s of CPU time), plus the reference's kernels.cl run on the
+    host (its OpenCL kernel, work-groups concurrent) as a second figure."""
+    score = NumbaScoring(W)
+    score(X[:64])
     t0 = time.perf_counter()
-    while True:
-        _score_sample(O, kind, W, th, sample)
-        done += sample
-        if time.perf_counter() - t0 > min(max_seconds, 10.0) or done >= 8 * sample:
-            break
+    score(X[:sample])
     dt = time.perf_counter() - t0
-    cores = os.cpu_count() or 1
-    how = ("the reference's calculate_cut (kernels.cl:44-94) compiled for the host, "
-           "run as 160 work-items in groups of 32 threads") if kind == "reference" else (
-           "the oracle's C port of calculate_cut, OpenMP over candidates")
-    return {
-        "value": done / dt,
+    out = {
+        "value": sample / dt,
         "unit": UNIT,
-        "cores": min(cores, 32) if kind == "reference" else cores,
-        "kind": kind,
-        "sample": f"{done} candidates of n={W.shape[0]} ({sample} per call): {how}",
+        "cores": score.cores,
+        "kind": "port",
+        "sample": f"{sample} of the batch's candidates (n={W.shape[0]}) in one call: {score.kind_text}",
     }
+    try:
+        O, kind = _emulator_or_c_port()
+        th = O.pack32(X[:256])
+        _kernels_cl_sample(O, kind, W, th[:32], 32)
+        t0 = time.perf_counter()
+        _kernels_cl_sample(O, kind, W, th, 256)
+        dt = time.perf_counter() - t0
+        out["kernels_cl_on_host"] = {
+            "value": 256 / dt,
+            "unit": UNIT,
+            "kind": kind,
+            "sample": "256 candidates: the reference's calculate_cut (kernels.cl:44-94) compiled for the host, "
+                      "160 work-items in groups of 32 threads, all groups at once" if kind == "reference" else
+                      "256 candidates: the oracle's C port of calculate_cut",
+        }
+    except Exception as ex:  # pragma: no cover
+        out["kernels_cl_on_host"] = {"unavailable": str(ex)}
+    return out
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the reference's CPU scoring of this workload (restated
+    in the oracle, see NumbaScoring) on all host threads; each step scores a
+    bounded sample of the step's batch. Rank 0 alone runs it."""
     if rank != 0:
         return 0
     W = make_graph()
-    X = np.random.default_rng(1000).random((256, N_NODES)) < 0.5
-    O, kind = _ref_or_port()
-    sample = 256
-    th = O.pack32(X[:sample])
+    sample = 2048
+    X = make_batch(0, sample)
+    score = NumbaScoring(W)
     for _ in range(max(1, args.warmup)):
-        _score_sample(O, kind, W, th[:32], 32)
+        score(X[:128])
     t_steps = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        _score_sample(O, kind, W, th, sample)
+        score(X)
         t_steps.append(time.perf_counter() - t0)
     ms = 1000.0 * float(np.mean(t_steps))
     value = sample / (ms / 1000.0)
-    cores = os.cpu_count() or 1
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -221,15 +269,13 @@ def run_reference(args, rank, world):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": workload_config({"reference_sample": f"{sample} of the {BATCH} candidates per step"}),
+        "config": workload_config(),
         "cpu_baseline": {
             "value": value,
             "unit": UNIT,
-            "cores": min(cores, 32) if kind == "reference" else cores,
-            "kind": kind,
-            "sample": f"{sample} candidates per step: " + (
-                "the reference's calculate_cut (kernels.cl:44-94) compiled for the host, 160 work-items in groups of 32 threads, plus its selection"
-                if kind == "reference" else "the oracle's C port of calculate_cut and its selection, OpenMP over candidates"),
+            "cores": score.cores,
+            "kind": "port",
+            "sample": f"{sample} of the {BATCH} candidates of a batch per step (the rate is per candidate): {score.kind_text}",
         },
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -286,6 +332,92 @@ def time_to_best(n=8192, starts=32, cluster=8):
         "batched_status": int(status.item()),
         "reaches_plain_best": e64 >= e_plain * (1.0 - 1e-5),
         "speedup": t_plain / t_batched,
+    }
+
+
+def time_to_best_learned(n=8192, starts=32, cluster=8, rounds=4, kick=64, temperature=3.0):
+    """The batched + learned form on SK n=8192 against the plain GPU form's
+    best energy. Stages, each timed on the host clock after a device sync:
+      1. cluster ascent from `starts` random states (one launch);
+      2. the network's proposals on each task's optimum (forward per task,
+         kick distributions by pqi_mpnn_kick_cdf);
+      3. `rounds` of the batched iterated search from those optima with
+         learned kicks.
+    time_to_plain_best is the elapsed time at the end of the first stage whose
+    running best reaches the plain form's best (None if none does). Beside
+    stage 3, the same search with uniform kicks from the same optima, seeds
+    and budget: what the network adds over the method without it."""
+    import importlib
+
+    import torch
+
+    from pyqrackising_b200 import learned as L
+    from pyqrackising_b200 import workloads as wl
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    SG = importlib.import_module("pyqrackising_b200.spin_glass_solver")
+    W = wl.sherrington_kirkpatrick(n, seed=1)
+    dg = DeviceGraph(W)
+    net = L.ProposalNet.load(os.path.join(REPO, "pyqrackising_b200", "weights", "proposal_net.pt"))
+    start = np.random.default_rng(0).random(n) < 0.5
+    bs = BatchedSearch([dg])
+    bsT = BatchedSearch([dg] * starts)  # one descriptor (and proposal) per task
+    tasks = [0] * starts
+    w0 = bs.random_states(tasks, seed=7)
+    # untimed warm run of every stage (module load, workspaces, attributes)
+    SG.local_search(dg, start, True, n * n, 148, 148, 0.0)
+    vA, wA, _, _ = bs.cluster_ascent(tasks, w0, True, cluster_size=cluster)
+    cdf, off = L.task_proposals(net, dg, wA, temperature=temperature)
+    bsT.run(list(range(starts)), wA.reshape(-1).contiguous(), True, rounds=1, kick=kick, seed=1,
+            kick_cdf=cdf, cdf_offset=off)
+    torch.cuda.synchronize()
+
+    t0 = time.perf_counter()
+    words, _ = SG.local_search(dg, start, True, n * n, 148, 148, 0.0)
+    _, e_plain = dg.rescore(words)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    e_plain = float(e_plain.item())
+
+    def reached(v):
+        return v >= e_plain * (1.0 - 1e-5) if e_plain >= 0 else v >= e_plain * (1.0 + 1e-5)
+
+    t0 = time.perf_counter()
+    vA, wA, _, _ = bs.cluster_ascent(tasks, w0, True, cluster_size=cluster)
+    b1 = float(vA.max().item())
+    t1 = time.perf_counter() - t0
+    cdf, off = L.task_proposals(net, dg, wA, temperature=temperature)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter() - t0
+    A = wA.reshape(-1).contiguous()
+    vP, wP, _, sP = bsT.run(list(range(starts)), A, True, rounds=rounds, kick=kick, seed=3, kick_cdf=cdf,
+                            cdf_offset=off)
+    b3 = float(vP.max().item())
+    t3 = time.perf_counter() - t0
+    ta = time.perf_counter()
+    vU, _, _, _ = bs.run(tasks, A, True, rounds=rounds, kick=kick, seed=3)
+    bU = float(vU.max().item())
+    t_uniform = time.perf_counter() - ta
+    best = int(torch.argmax(vP).item())
+    _, e64 = dg.rescore(wP[best].contiguous())
+    ttb = t1 if reached(b1) else (t3 if reached(max(b1, b3)) else None)
+    return {
+        "workload": f"SK n={n}, J~N(0,1)/sqrt(n) float32, is_spin_glass; plain: local-search loop from 1 start; "
+                    f"batched + learned: {starts} starts, cluster ascent ({cluster} CTAs per start), the trained "
+                    f"network's per-task proposals (T={temperature}), {rounds} rounds of batched iterated search "
+                    f"with {kick} learned kicks per round",
+        "plain_s": t_plain,
+        "plain_energy": e_plain,
+        "stage_ascent_s": t1, "stage_ascent_best": b1,
+        "stage_proposals_s": t2 - t1,
+        "stage_learned_search_s": t3 - t2, "stage_learned_search_best": b3,
+        "uniform_search_best": bU, "uniform_search_s": t_uniform,
+        "learned_minus_uniform": b3 - bU,
+        "best_energy_rel_err_vs_fp64": abs(b3 - float(e64.item())) / max(abs(float(e64.item())), 1e-300),
+        "status": int(sP.item()),
+        "time_to_plain_best_s": ttb,
+        "speedup": (t_plain / ttb) if ttb else None,
     }
 
 
@@ -433,7 +565,7 @@ def batched_leg(graphs=512, seeds=256):
     }
 
 
-def flip_bandwidth_leg(n=8192, tasks=1776, fields="f64"):
+def flip_bandwidth_leg(n=8192, tasks=1776, fields="auto"):
     """Flip updates on the SK spin glass (W = 256 MB float32, larger than L2):
     many starts of the batched ascent at once; each accepted flip reads one W
     row (n * 4 bytes) and updates the task's n local fields. The starting
@@ -460,7 +592,7 @@ def flip_bandwidth_leg(n=8192, tasks=1776, fields="f64"):
     b.synchronize()
     t_init = a.elapsed_time(b)
     a.record()
-    _, _, f2, st = bs.run(tg, w0, True, rounds=0, flip_budget=1 + 2048, fields=fields)
+    v2, b2, f2, st = bs.run(tg, w0, True, rounds=0, flip_budget=1 + 2048, fields=fields)
     b.record()
     b.synchronize()
     t_all = a.elapsed_time(b)
@@ -468,8 +600,15 @@ def flip_bandwidth_leg(n=8192, tasks=1776, fields="f64"):
     dt = (t_all - t_init) / 1e3
     hbm, _, src = peaks()
     gbs = flips * n * 4 / dt / 1e9
+    # the tracked values against float64 re-scoring of the returned states
+    pick = list(range(0, tasks, max(1, tasks // 16)))
+    _, e64 = dg.rescore(b2[pick].contiguous(), rows=len(pick))
+    tracked = v2[pick]
+    rel = float(((tracked - e64).abs() / e64.abs().clamp_min(1e-300)).max().item())
+    used = fields if fields != "auto" else ("f32" if n > 4096 else "f64")
     return {
-        "workload": f"SK n={n} float32, {tasks} starts of the batched ascent, 2048 flips each after the starting fields (timed apart and subtracted), {fields} local fields",
+        "workload": f"SK n={n} float32, {tasks} starts of the batched ascent, 2048 flips each after the starting fields (timed apart and subtracted), {used} local fields, float64 acceptance and running value",
+        "tracked_value_rel_err_vs_fp64": rel,
         "flips": flips,
         "flips_per_s": flips / dt,
         "row_bytes_per_flip": n * 4,
@@ -480,14 +619,285 @@ def flip_bandwidth_leg(n=8192, tasks=1776, fields="f64"):
     }
 
 
+# ----------------------------------------------------------------------------
+# Legs outside the headline line: `python bench.py --leg NAME [NAME ...]` runs
+# the named legs alone and prints one JSON line per measurement (device time
+# by CUDA events on the launching stream; L2 flushed where W exceeds it).
+#
+#   double   one double-bit-flip pass (kernels.cl:150-231 semantics, from
+#            maintained gains) on SK n=8192 float32 and ER(2048, 0.5) int8
+#   gray     one Gray-code search (kernels.cl:877-978 semantics) from a
+#            single-flip local optimum: SK n=8192 (n^2 iterations, 148 seeds)
+#            and ER(1024, 0.5) (n^2/16 iterations)
+#   tfim     the TFIM sampler alone (3-regular and ER n=2048, quality 6:
+#            65,536 shots) and maxcut_tfim end to end on ER(1024, 0.5), q=2
+#   sparse   spin_glass_solver_sparse on G(16384, 0.01) N(0,1) next to the
+#            dense solver on the same matrix
+#   bnb      solve_maxcut_bnb on 3-regular +-1 graphs, n = 28 and 32
+#   flips    a short batched ascent on SK n=8192 (444 starts, 64 flips each,
+#            float64 fields; a small case for profiling the flip phase)
+#   cluster  a cluster ascent on SK n=8192 (8 starts, 8-CTA clusters), checked
+#            against the CTA-per-task form
+#   mpnn     one proposal-network forward and backward on G(16384, 0.01)
+# A leg exits non-zero when its result disagrees with its check.
+
+_flush_buf = None
+
+
+def _flush_l2():
+    """Write 256 MB (twice the L2) so the next launch starts cold."""
+    import torch
+
+    global _flush_buf
+    if _flush_buf is None:
+        _flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    _flush_buf.fill_(1)
+
+
+def _timed(fn, reps, flush=True):
+    """Mean device time (ms) of fn() over reps launches."""
+    import torch
+
+    total = 0.0
+    for _ in range(reps):
+        if flush:
+            _flush_l2()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        total += a.elapsed_time(b)
+    return total / reps
+
+
+def _emit(**kw):
+    print(json.dumps(kw), flush=True)
+
+
+def _local_optimum(dg, seed, spin=True):
+    """Random state taken to a single-flip local optimum with the device descent.
+    The words hold ceil(n/32) + 1 int32, so they also read as ceil(n/64) 64-bit words."""
+    from pyqrackising_b200 import device as D
+    from pyqrackising_b200 import workloads as wl
+
+    words = dg.pack(wl.random_bits(dg.n, seed))
+    _, g64 = dg.gains(words)
+    Gf, Lf = D.geometry(min(D.WORK_GROUP_MULTIPLE, dg.n), dg.n, D.max_gpu_proc_elem())
+    while True:
+        _, _, rc = dg.single_descent(words, g64, spin, Gf, Lf, 1 << 16)
+        if rc != 3:
+            break
+    return words, g64, Gf, Lf
+
+
+def leg_double():
+    from pyqrackising_b200 import device as D
+    from pyqrackising_b200 import workloads as wl
+
+    hbm, _, src = peaks()
+    for name, W, spin in (("SK n=8192 float32", wl.sherrington_kirkpatrick(8192, seed=1), True),
+                          ("ER(2048, 0.5) int8", wl.erdos_renyi(2048, 0.5, seed=1), False)):
+        dg = D.DeviceGraph(W)
+        n = dg.n
+        words, g64, Gf, Lf = _local_optimum(dg, 3, spin)
+        for _ in range(3):
+            dg.double_bit_flips(words, g64, spin, Gf, Lf)
+        ms = _timed(lambda: dg.double_bit_flips(words, g64, spin, Gf, Lf), 20)
+        pairs = n * (n - 1) // 2
+        wbytes = pairs * (1 if dg.is_integer else 4)
+        _emit(leg="double", graph=name, n=n, ms_per_pass=round(ms, 4), pairs_per_s=pairs / ms * 1e3,
+              w_bytes=wbytes, gbs=round(wbytes / ms / 1e6, 1), hbm_frac=round(wbytes / ms / 1e6 / hbm, 3),
+              peak_basis=f"{src} HBM copy bandwidth {hbm} GB/s", l2_flushed=True)
+
+
+def leg_gray():
+    from pyqrackising_b200 import device as D
+    from pyqrackising_b200 import workloads as wl
+
+    mpe = D.max_gpu_proc_elem()
+    for name, W, spin, iters, seeds in (
+        ("SK n=8192 float32", wl.sherrington_kirkpatrick(8192, seed=1), True, 8192 * 8192, mpe),
+        ("ER(1024, 0.5) float32", wl.erdos_renyi(1024, 0.5, seed=1), False, 1024 * 1024 // 16, mpe),
+    ):
+        import torch
+
+        dg = D.DeviceGraph(W)
+        n = dg.n
+        words, g64, _, _ = _local_optimum(dg, 4, spin)
+        bound = (iters + seeds - 1) // seeds
+        for _ in range(2):
+            dg.gray(words, g64, spin, bound, seeds)
+        ms = _timed(lambda: dg.gray(words, g64, spin, bound, seeds), 5)
+        blocks = dg.n64
+        positions = sum(((bound - 1 - s) // seeds + 1) * blocks for s in range(seeds) if bound > s)
+        _, eout = dg.gray(words, g64, spin, bound, seeds)
+        torch.cuda.synchronize()
+        _emit(leg="gray", graph=name, n=n, seeds=seeds, iterations=iters, ms_per_search=round(ms, 3),
+              positions=positions, positions_per_s=positions / ms * 1e3,
+              improving_seeds=int((eout > 0).sum().item()))
+
+
+def leg_tfim():
+    import importlib
+
+    import torch
+
+    from pyqrackising_b200 import device as D
+    from pyqrackising_b200 import workloads as wl
+
+    MT = importlib.import_module("pyqrackising_b200.maxcut_tfim")
+    for name, W in (("3-regular n=2048 +-1", wl.regular_pm1_fast(2048, seed=5)),
+                    ("ER(2048, 0.5)", wl.erdos_renyi(2048, 0.5, seed=1))):
+        dg = D.DeviceGraph(W)
+        _, _, cum = MT.hamming_cdf(dg, 6, 8.0, 8.0)
+        shots = ((max(1, (2048 << 6) >> 1) + 31) >> 5) << 5
+        buf = MT.sample_batch(dg, cum, shots, 5.0, 1, 0)
+        for r in range(2):
+            MT.sample_batch(dg, cum, shots, 5.0, 1, r, out=buf)
+        ms = _timed(lambda: MT.sample_batch(dg, cum, shots, 5.0, 1, 7, out=buf), 3, flush=False)
+        bits = dg.unpack(buf, rows=shots)
+        _emit(leg="tfim_sampler", graph=name, quality=6, shots=shots, ms_per_round=round(ms, 3),
+              shots_per_s=shots / ms * 1e3, mean_selected_per_shot=float(bits.sum()) / shots,
+              note="W (16 MB) is L2-resident; a selected node is a picked or underflowed weight")
+    W1 = wl.erdos_renyi(1024, 0.5, seed=1)
+    MT.set_seed(0)
+    MT.maxcut_tfim(W1, quality=2)
+    runs = []
+    for seed in range(5):
+        MT.set_seed(seed)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, cut, _ = MT.maxcut_tfim(W1, quality=2)
+        torch.cuda.synchronize()
+        runs.append((time.perf_counter() - t0, cut))
+    MT.set_seed(None)
+    _emit(leg="maxcut_tfim", graph="ER(1024, 0.5)", quality=2, wall_s=[round(t, 4) for t, _ in runs],
+          cuts=[c for _, c in runs], note="host wall time per call, W upload and preparation included")
+
+
+def leg_sparse():
+    import scipy.sparse as sp
+    import torch
+
+    from pyqrackising_b200 import spin_glass_solver, spin_glass_solver_sparse
+    from pyqrackising_b200 import workloads as wl
+
+    W = wl.gnp_weighted(16384, 0.01, seed=1, dist="normal")
+    G = sp.csr_matrix(np.triu(W, 1))
+    best = "".join("1" if b else "0" for b in wl.random_bits(16384, 9))
+    out = {}
+    for name, fn, arg in (("sparse", spin_glass_solver_sparse, G), ("dense", spin_glass_solver, W)):
+        fn(arg, best_guess=best)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, cut, _, energy = fn(arg, best_guess=best)
+        torch.cuda.synchronize()
+        out[name] = (time.perf_counter() - t0, cut, energy)
+    _emit(leg="sparse", graph="G(16384, 0.01) N(0,1)", nnz_upper=int(G.nnz),
+          sparse_s=round(out["sparse"][0], 3), dense_s=round(out["dense"][0], 3),
+          sparse_energy=out["sparse"][2], dense_energy=out["dense"][2],
+          note="same best_guess; host wall time per call, coordinate upload / W upload included")
+
+
+def leg_bnb():
+    import contextlib
+    import io
+    import re
+
+    from pyqrackising_b200 import solve_maxcut_bnb
+    from pyqrackising_b200 import workloads as wl
+
+    warm = solve_maxcut_bnb(wl.regular_pm1_fast(12, seed=3), best_guess="0" * 12, verbose=False)
+    assert warm[4]
+    for n in (28, 32):
+        W = wl.regular_pm1_fast(n, seed=3)
+        rng = np.random.default_rng(1)
+        guess = "".join("1" if b else "0" for b in rng.random(n) < 0.5)
+        for cap in (64, 4096):
+            buf = io.StringIO()
+            t0 = time.perf_counter()
+            with contextlib.redirect_stdout(buf):
+                bits, cut, _, _, certified = solve_maxcut_bnb(W, best_guess=guess, verbose=True, batch_size=cap)
+            dt = time.perf_counter() - t0
+            m = re.search(r"Nodes explored: (\d+)\s+\|\s+Pruned: (\d+)", buf.getvalue())
+            _emit(leg="bnb", graph=f"3-regular n={n} +-1", batch_size=cap, wall_s=round(dt, 3), cut=cut,
+                  certified=bool(certified), nodes=int(m.group(1)), pruned=int(m.group(2)),
+                  nodes_per_s=round(int(m.group(1)) / dt))
+
+
+def leg_flips(tasks=444, budget=64, fields="f64"):
+    import torch
+
+    from pyqrackising_b200 import workloads as wl
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    bs = BatchedSearch([DeviceGraph(wl.sherrington_kirkpatrick(8192, seed=1))])
+    tg = torch.zeros(tasks, dtype=torch.int32, device="cuda")
+    w0 = bs.random_states(np.zeros(tasks, dtype=np.int32), seed=5)
+    for _ in range(2):
+        v, _, flips, st = bs.run(tg, w0, True, rounds=0, flip_budget=budget, fields=fields)
+    torch.cuda.synchronize()
+    _emit(leg="flips", tasks=tasks, flip_budget=budget, fields=fields, flips=int(flips.item()), status=int(st.item()))
+    if int(st.item()) not in (0, 3):  # 3: the flip budget ran out, as intended
+        raise SystemExit(1)
+
+
+def leg_cluster(n=8192, starts=8):
+    import torch
+
+    from pyqrackising_b200 import workloads as wl
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    bs = BatchedSearch([DeviceGraph(wl.sherrington_kirkpatrick(n, seed=1))])
+    tasks = [0] * starts
+    w0 = bs.random_states(tasks, seed=7)
+    v, best, flips, st = bs.cluster_ascent(tasks, w0, True, cluster_size=8)
+    v2, best2, flips2, st2 = bs.run(tasks, w0, True, rounds=0)
+    torch.cuda.synchronize()
+    ok = torch.equal(best, best2) and int(st.item()) == 0
+    _emit(leg="cluster", flips=int(flips.item()), best=float(v.max()), matches_batched=ok)
+    if not ok:
+        raise SystemExit(1)
+
+
+def leg_mpnn(n=16384):
+    import torch
+
+    from pyqrackising_b200 import learned as L
+    from pyqrackising_b200 import workloads as wl
+    from pyqrackising_b200.device import DeviceGraph
+
+    dg = DeviceGraph(wl.gnp_weighted(n, 0.01, seed=5, dist="normal"))
+    ctx = L.GraphContext(dg)
+    net = L.ProposalNet(seed=1)
+    F = ctx.features(dg.pack(np.random.default_rng(1).random(n) < 0.5))
+    logits, cache = net.forward(ctx, F)
+    _, dl, _ = net.loss_grad(logits, torch.full((n,), 1.0 / n, device="cuda"))
+    net.backward(ctx, cache, dl)
+    torch.cuda.synchronize()
+    ok = bool(torch.isfinite(logits).all().item()) and bool(torch.isfinite(net.g).all().item())
+    _emit(leg="mpnn", n=n, finite=ok)
+    if not ok:
+        raise SystemExit(1)
+
+
+LEGS = {"double": leg_double, "gray": leg_gray, "tfim": leg_tfim, "sparse": leg_sparse, "bnb": leg_bnb,
+        "flips": leg_flips, "cluster": leg_cluster, "mpnn": leg_mpnn}
+
+
 def make_graph():
     from pyqrackising_b200 import workloads as wl
 
     return wl.erdos_renyi(N_NODES, EDGE_P, seed=1)
 
 
-def make_batch(seed):
-    return np.random.default_rng(1000 + seed).random((BATCH, N_NODES)) < 0.5
+def make_batch(seed, rows=BATCH):
+    """Candidates of batch `seed` (seeded uniform bits); the first `rows` rows
+    of the full batch."""
+    return np.random.default_rng(1000 + seed).random((rows, N_NODES)) < 0.5
 
 
 def main():
@@ -498,7 +908,17 @@ def main():
     ap.add_argument("--no-ttb", action="store_true", help="skip the SK n=8192 time-to-best leg")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-uneven and flip-bandwidth legs")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--leg", nargs="+", choices=sorted(LEGS), help="run only these legs (one GPU), one JSON line each")
+    ap.add_argument("--leg-args", nargs="*", default=[], help="positional arguments of a single leg (flips: tasks budget f64|f32)")
     args = ap.parse_args()
+    if args.leg:
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        for name in args.leg:
+            conv = [int(a) if a.lstrip("-").isdigit() else a for a in args.leg_args]
+            LEGS[name](*conv)
+        return 0
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -572,10 +992,16 @@ def main():
         # stream (double-buffered, so step i+1's copy overlaps step i's
         # scoring), scores it, and reads the (value, index) pair back.
         e2e_ms = e2e_pipeline(dg, batches_host, batches[0], G, L, args.steps, args.warmup)
-    if dist:
-        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device=dg.device)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_ms = float(t[0]), float(t[1])
+    # the slowest rank's device time; then the batches' best candidate over
+    # ranks (each rank scored its own share of the candidates): one exchange
+    from pyqrackising_b200 import distributed as DI
+
+    cdev = DI.collective_device(dist)
+    total_ms = DI.max_over_ranks(total_ms, dist, cdev)
+    e2e_ms = DI.max_over_ranks(e2e_ms, dist, cdev)
+    _, be, bi = dg.calculate_cut(batches[0], BATCH, False, G, L, energies=False)
+    win_words = batches[0].view(BATCH, -1)[int(bi.item())]
+    best_value, best_rank, _ = DI.best_over_ranks(float(be.item()), win_words, dist, cdev)
 
     ms_per_step = total_ms / args.steps
     value = world * BATCH * args.steps / (total_ms / 1000.0)
@@ -621,23 +1047,25 @@ def main():
             "kernel_ms": kernel_ms,
             "algorithmic_ops_per_launch": ops,
         },
-        # per step: expand_pm1_kernel + score_tc_kernel (the L2 flush is torch's fill)
-        "gpu_launches": 2 * args.steps,
+        # per step: score_tc_kernel (the L2 flush is torch's fill)
+        "gpu_launches": args.steps,
+        "best_over_ranks": {"value": best_value, "rank": best_rank},
         "wall_s_timed_loop": wall,
     }
     if rank == 0:
         line["clocks"] = clocks.summary()
         if world == 1 and not args.no_ttb:
             line["time_to_best"] = time_to_best()
+            line["time_to_best_learned"] = time_to_best_learned()
         if world == 1 and not args.no_batched:
             line["plain_small"] = plain_small_leg()
             line["batched"] = batched_leg()
             line["learned"] = learned_leg()
             line["flip_updates"] = flip_bandwidth_leg()
-            line["flip_updates_f32_fields"] = flip_bandwidth_leg(fields="f32")
+            line["flip_updates_f64_fields"] = flip_bandwidth_leg(fields="f64")
         if world == 1:
             try:
-                line["cpu_baseline"] = cpu_baseline(W, make_batch(0))
+                line["cpu_baseline"] = cpu_baseline(W, make_batch(0, 2048))
             except Exception as ex:  # pragma: no cover
                 line["cpu_baseline"] = {"unavailable": str(ex)}
         print(json.dumps(line), flush=True)
