@@ -85,15 +85,26 @@ class BatchedSearch:
     def run(self, task_graph, init_words: torch.Tensor, is_spin_glass: bool, rounds: int = 0, kick: int = 4,
             seed: int = 0, kick_cdf: torch.Tensor | None = None, cdf_offset: torch.Tensor | None = None,
             flip_budget: int | None = None, variant: str = "cta", warps_per_sm: int = 0, out=None,
-            fields: str = "f64"):
+            fields: str = "auto"):
         """Iterated local search of every task. variant: "cta" (one CTA of 256
         threads per task, any n), "cta128" / "cta64" (CTAs of 128 / 64 threads:
         two / four times the resident tasks, for small graphs) or "warp" (one
-        warp per task, max_n <= 1024); all give the same results. fields: "f64" (default) or "f32" (CTA form, float
-        graphs: float32 local fields, more resident tasks per SM; rounding can
-        change trajectories). `out` = (best_states, best_values, flips, status)
-        device buffers to fill (for CUDA-graph capture); flips and status are
-        accumulated into, so zero them between uses."""
+        warp per task, max_n <= 1024); all give the same results.
+
+        fields (CTA forms, float graphs): "f64" keeps float64 local fields;
+        "f32" keeps float32 local fields (half the shared memory, four resident
+        tasks per SM instead of three) that only rank the candidates: the
+        starting value is summed in float64, and each flip's float64 gain,
+        summed over the flipped row in the same pass, decides its acceptance
+        and is what the running value adds, so every accepted flip improves
+        the float64 objective and the returned value is float64-exact. The
+        ranking can differ from float64 fields' where gains agree to float32
+        rounding. "auto" (default): "f32" above 4096 nodes, else "f64".
+        Integer graphs are exact either way.
+
+        `out` = (best_states, best_values, flips, status) device buffers to
+        fill (for CUDA-graph capture); flips and status are accumulated into,
+        so zero them between uses."""
         tg = task_graph if torch.is_tensor(task_graph) else torch.as_tensor(np.asarray(task_graph, dtype=np.int32)).to(self.device)
         tasks = int(tg.numel())
         if out is None:
@@ -115,8 +126,10 @@ class BatchedSearch:
             return best_values, best_states.view(tasks, self.pitch), flips, status
         if variant not in ("cta", "cta128", "cta64"):
             raise ValueError("variant must be 'cta', 'cta128', 'cta64' or 'warp'")
+        if fields == "auto":
+            fields = "f32" if self.kind != _lib.PQI_W_I8 and self.max_n > 4096 else "f64"
         if fields not in ("f64", "f32"):
-            raise ValueError("fields must be 'f64' or 'f32'")
+            raise ValueError("fields must be 'f64', 'f32' or 'auto'")
         if variant in ("cta128", "cta64"):
             _lib.call(
                 "pqi_batch_search_cta", D._ptr(self.desc), len(self.graphs), D._ptr(tg), D._ptr(init_words),
@@ -200,25 +213,45 @@ class BatchedSolver:
     threads per task, or one warp per task with an occupancy cap) on the
     group's tasks and keeps the fastest; `capture()` then records every launch of a step in one CUDA
     graph, so a step is one graph replay. Results are the best value and state
-    per graph over its seeds (reduced on the device).
+    per graph over its seeds.
+
+    Multi-GPU (``dist``, an initialised torch.distributed module, one process
+    per GPU): every rank runs the contiguous share [lo, hi) of each graph's
+    seeds (``distributed.shard_range``) with no collective in the search, and
+    ``results()`` exchanges once (``distributed.sharded_best``): per graph the
+    best value, then the lowest seed. Starting states are drawn for all seeds
+    and sliced, so a rank's starts are the ones a single rank would use; with
+    rounds = 0 the merged result equals the single-rank result. (With kicks,
+    the kick stream depends on the task's position in the rank's launch, and
+    ranks above 0 use the seed of ``distributed.shard_seed``.) dist=None is
+    the same code path with one rank.
     """
 
     FORMS = (("cta", 0), ("cta128", 0), ("cta64", 0), ("warp", 0), ("warp", 16), ("warp", 8))
 
     def __init__(self, graphs: list[D.DeviceGraph], seeds_per_graph: int, is_spin_glass: bool,
-                 rounds: int = 0, kick: int = 8, seed: int = 0, stream=None):
+                 rounds: int = 0, kick: int = 8, seed: int = 0, stream=None, dist=None):
+        from . import distributed as DI
+
         if seeds_per_graph < 1:
             raise ValueError("seeds_per_graph must be >= 1")
         self.graphs = graphs
         self.S = int(seeds_per_graph)
+        self.dist = dist
+        world, rank = DI.world_rank(dist)
+        if self.S < world:
+            raise ValueError("seeds_per_graph must be at least the world size")
+        self.lo, self.hi = DI.shard_range(self.S, rank, world)
+        self.S_local = self.hi - self.lo
         self.spin = bool(is_spin_glass)
-        self.rounds, self.kick, self.seed = int(rounds), int(kick), int(seed)
+        self.rounds, self.kick = int(rounds), int(kick)
+        self.seed = int(seed) if rank == 0 else DI.shard_seed(int(seed), rank)
         self.stream = stream
         self.groups = []
         for kind in sorted({g.w.kind for g in graphs}):
             idx = [i for i, g in enumerate(graphs) if g.w.kind == kind]
             bs = BatchedSearch([graphs[i] for i in idx], stream=stream)
-            tg = np.repeat(np.arange(len(idx), dtype=np.int32), self.S)
+            tg = np.repeat(np.arange(len(idx), dtype=np.int32), self.S_local)
             self.groups.append({
                 "kind": kind, "index": idx, "bs": bs,
                 "tg": torch.from_numpy(tg).to(bs.device),
@@ -272,11 +305,16 @@ class BatchedSolver:
             )
 
     def set_starts(self, seed: int):
-        """Fresh uniform random starting states for every task (device side)."""
+        """Fresh uniform random starting states for every task (device side):
+        drawn for all seeds of every graph, this rank's share kept."""
         if "init" not in self.groups[0]:
             self._buffers()
         for grp in self.groups:
-            grp["init"].copy_(grp["bs"].random_states(grp["tg"].cpu().numpy(), seed=seed))
+            bs = grp["bs"]
+            ng = len(grp["index"])
+            full = bs.random_states(np.repeat(np.arange(ng, dtype=np.int32), self.S), seed=seed)
+            share = full.view(ng, self.S, bs.pitch)[:, self.lo:self.hi].reshape(-1, bs.pitch)
+            grp["init"].copy_(share)
 
     def _launch_all(self):
         for grp in self.groups:
@@ -308,24 +346,37 @@ class BatchedSolver:
             self._launch_all()
 
     def results(self):
-        """(best value per graph [G] float64, best state words per graph, flips, status)."""
+        """(best value per graph [G] float64, best state words per graph, flips,
+        status), over all ranks when the solver is sharded: the per-seed results
+        of this rank's share go through ``distributed.sharded_best`` (one
+        exchange of values, one of the winners' words)."""
+        from . import distributed as DI
+
         G = len(self.graphs)
         dev = self.groups[0]["bs"].device
-        values = torch.empty(G, dtype=torch.float64, device=dev)
-        states = [None] * G
+        P = max(grp["bs"].pitch for grp in self.groups)
+        vals = np.empty((G, self.S_local), dtype=np.float64)
+        words = np.zeros((G, self.S_local, P), dtype=np.uint32)
         flips = 0
         status = 0
         for grp in self.groups:
             bs = grp["bs"]
             st, bv, fl, stt = grp["out"]
-            v = bv.view(-1, self.S)
-            best, arg = torch.max(v, dim=1)  # first maximum: the lowest seed on ties
-            idx = torch.as_tensor(grp["index"], device=dev)
-            values[idx] = best
-            words = st.view(-1, self.S, bs.pitch)
-            pick = words[torch.arange(v.shape[0], device=dev), arg]
-            for j, gi in enumerate(grp["index"]):
-                states[gi] = pick[j]
+            idx = np.asarray(grp["index"])
+            vals[idx] = bv.view(-1, self.S_local).cpu().numpy()
+            words[idx, :, : bs.pitch] = st.view(-1, self.S_local, bs.pitch).cpu().numpy().view(np.uint32)
             flips += int(fl.item())
             status = max(status, int(stt.item()))
+        cdev = DI.collective_device(self.dist)
+        best_v, _, best_w = DI.sharded_best(G, self.S, lambda lo, hi: (vals, words), self.dist, cdev)
+        world, _ = DI.world_rank(self.dist)
+        if world > 1:
+            tf = torch.tensor([flips], dtype=torch.int64, device=cdev)
+            ts = torch.tensor([status], dtype=torch.int64, device=cdev)
+            self.dist.all_reduce(tf, op=self.dist.ReduceOp.SUM)
+            self.dist.all_reduce(ts, op=self.dist.ReduceOp.MAX)
+            flips, status = int(tf.item()), int(ts.item())
+        pitch = {gi: grp["bs"].pitch for grp in self.groups for gi in grp["index"]}
+        values = torch.from_numpy(best_v).to(dev)
+        states = [torch.from_numpy(best_w[gi, : pitch[gi]].view(np.int32).copy()).to(dev) for gi in range(G)]
         return values, states, flips, status
