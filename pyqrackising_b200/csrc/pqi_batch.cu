@@ -125,12 +125,20 @@ __device__ __forceinline__ unsigned long long bmax_key(unsigned long long key) {
 // chosen by the pass parity; after the barrier every warp reduces the slots
 // itself, so the next pass starts without a second barrier (a warp can be at
 // most one pass ahead of another, which writes the other slot array).
-// k < 0: no flip, only the selection. Returns the key and the exact gain.
+// k < 0: no flip, only the selection. Returns the key and the exact gain of
+// the selected node. With float32 fields the pass also sums, in float64,
+// x_v W_kv over row k as it streams by: *out_gx = x_k sum_v x_v W_kv is then
+// the float64 gain of the flipped node k (its acceptance test and the running
+// value use it; the float32 fields only rank the candidates). The partial sums
+// ride on the same barrier as the selection.
 template <typename WT, typename GT, int CH, bool STG, int BT>
 __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k, int xk,
                                                 unsigned long long (*red_key)[8],
-                                                double (*red_g)[8], int par,
-                                                unsigned long long* out_key, double* out_g) {
+                                                double (*red_g)[8], double (*red_x)[8], int par,
+                                                unsigned long long* out_key, double* out_g,
+                                                double* out_gx) {
+  constexpr bool GX = std::is_same<GT, float>::value;
+  double px = 0.0;  // this thread's share of sum_v x_v W_kv (GX)
   const int n = c.n;
   const GT coef = (k >= 0) ? (xk ? (GT)-2 : (GT)2) : (GT)0;
   const WT* __restrict__ row = c.W + (size_t)(k >= 0 ? k : 0) * c.ld;
@@ -160,6 +168,10 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
           g0[BT * i] = y;
         }
         const int xv = (word >> (v & 31)) & 1;
+        if constexpr (GX) {
+          // bit k may already be toggled here; W_kk = 0 in the prepared copy
+          if (k >= 0) px += xv ? (double)w4[i] : -(double)w4[i];
+        }
         // v ascends within a thread: strict '>' keeps the lowest node
         if constexpr (std::is_same<GT, float>::value) {
           const float gv = xv ? y : -y;
@@ -257,6 +269,10 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   const unsigned long long wk = bmax_key(key);
   if (lane == 0) red_key[par][warp] = wk;
   if (key != 0ull && key == wk) red_g[par][warp] = bg;
+  if constexpr (GX) {
+    for (int o = 16; o > 0; o >>= 1) px += __shfl_xor_sync(0xFFFFFFFFu, px, o);
+    if (lane == 0) red_x[par][warp] = px;
+  }
   __syncthreads();
   const int nwarps = blockDim.x >> 5;
   const unsigned long long sk = lane < nwarps ? red_key[par][lane] : 0ull;
@@ -265,6 +281,14 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   const uint32_t src = __ballot_sync(0xFFFFFFFFu, sk == gk && gk != 0ull);
   *out_g = __shfl_sync(0xFFFFFFFFu, sg, src ? __ffs(src) - 1 : 0);
   *out_key = gk;
+  if constexpr (GX) {
+    // every warp sums the slots in the same order: one value CTA-wide
+    double sx = 0.0;
+    for (int i = 0; i < nwarps; ++i) sx += red_x[par][i];
+    *out_gx = xk ? sx : -sx;
+  } else {
+    *out_gx = 0.0;
+  }
 }
 
 // F32: float graphs keep float32 local fields (half the shared memory and
@@ -289,6 +313,7 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
   __shared__ double red[32];
   __shared__ unsigned long long red_key[2][8];
   __shared__ double red_g[2][8];
+  __shared__ double red_x[2][8];
   for (int task = blockIdx.x; task < tasks; task += gridDim.x) {
     const BatchGraph G = graphs[task_graph[task]];
     const int n = G.n, n32 = (n + 31) >> 5;
@@ -316,36 +341,46 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
     // +-W_u to each thread's own nodes (rows ascending, CH groups of four per
     // pass in registers): a memory stream with few instructions, which leaves
     // the SM to the flips of the other resident tasks.
+    // Float32 fields are summed in float64 and rounded once when stored; the
+    // thread that stores field v also adds x_v y_v (float64) to its share of
+    // q = x^T W x, so the starting value is the float64 one for every field type.
+    typedef typename std::conditional<F32, double, GT>::type AT;
+    double qpart = 0.0;
+    auto store_field = [&](int v, AT acc) {
+      c.g[fpos<BT>(v)] = (GT)acc;
+      qpart += ((c.bits[v >> 5] >> (v & 31)) & 1) ? (double)acc : -(double)acc;
+    };
     if (G.adj_ptr) {
       for (int v = threadIdx.x; v < n; v += blockDim.x) {
-        GT acc = 0;
+        AT acc = 0;
         const long long e1 = G.adj_ptr[v + 1];
         for (long long e = G.adj_ptr[v]; e < e1; ++e) {
           const int u = G.adj_col[e];
           if (u == v) continue;
-          const GT w = (GT)G.adj_val[e];
+          const AT w = (AT)G.adj_val[e];
           acc += ((c.bits[u >> 5] >> (u & 31)) & 1) ? w : -w;
         }
-        c.g[fpos<BT>(v)] = acc;
+        store_field(v, acc);
       }
     } else if (n < 2048) {
       const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
       for (int k = threadIdx.x >> 5; k < n; k += warps) {
         const WT* row = c.W + (size_t)k * c.ld;
-        GT acc = 0;
+        AT acc = 0;
         for (int v = lane; v < n; v += 32) {
-          const GT w = (GT)row[v];
+          const AT w = (AT)row[v];
           acc += ((c.bits[v >> 5] >> (v & 31)) & 1) ? w : -w;
         }
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
-        if (lane == 0) c.g[fpos<BT>(k)] = acc;
+        if (lane == 0) store_field(k, acc);
       }
     } else {
       // at most two groups per pass: eight accumulators keep the register
-      // budget of three resident CTAs per SM
-      constexpr int CI = CH > 2 ? 2 : CH;
+      // budget of three resident CTAs per SM (one group with float64
+      // accumulators for float32 fields: four resident CTAs)
+      constexpr int CI = F32 ? 1 : (CH > 2 ? 2 : CH);
       for (int base = 4 * threadIdx.x; base < n; base += CI * 4 * BT) {
-        GT acc[4 * CI];
+        AT acc[4 * CI];
 #pragma unroll
         for (int e = 0; e < 4 * CI; ++e) acc[e] = 0;
 #pragma unroll 2
@@ -370,7 +405,7 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
                 for (int i = 0; i < 4; ++i) w4[i] = (v + i < n) ? __ldg(row + v + i) : (WT)0;
               }
 #pragma unroll
-              for (int i = 0; i < 4; ++i) acc[4 * j + i] += xu ? (GT)w4[i] : -(GT)w4[i];
+              for (int i = 0; i < 4; ++i) acc[4 * j + i] += xu ? (AT)w4[i] : -(AT)w4[i];
             }
           }
         }
@@ -379,15 +414,13 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int v = base + j * 4 * BT + i;
-            if (v < n) c.g[fpos<BT>(v)] = acc[4 * j + i];
+            if (v < n) store_field(v, acc[4 * j + i]);
           }
       }
     }
     __syncthreads();
     // q = x^T W x = sum_k x_k y_k; value from q
-    double part = 0.0;
-    for (int v = threadIdx.x; v < n; v += blockDim.x)
-      part += ((c.bits[v >> 5] >> (v & 31)) & 1) ? (double)c.g[fpos<BT>(v)] : -(double)c.g[fpos<BT>(v)];
+    double part = qpart;
     for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xFFFFFFFFu, part, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = part;
     __syncthreads();
@@ -400,9 +433,9 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
     unsigned long long nflips = 0;
     int timeout = 0;
     unsigned long long key;
-    double gk;
+    double gk, gx;
     int par = 0;
-    flip_and_select<WT, GT, CH, STG, BT>(c, -1, 0, red_key, red_g, par, &key, &gk);
+    flip_and_select<WT, GT, CH, STG, BT>(c, -1, 0, red_key, red_g, red_x, par, &key, &gk, &gx);
     par ^= 1;
     for (int r = 0; r <= rounds; ++r) {
       // steepest ascent: flip the best node while its gain is positive
@@ -413,9 +446,23 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
           break;
         }
         const int k = (int)(0x3FFFFFFFu - (((uint32_t)key) >> 1));
-        val += scale * gk;  // exact gain of k before the flip
-        flip_and_select<WT, GT, CH, STG, BT>(c, k, (int)(key & 1ull), red_key, red_g, par, &key, &gk);
-        par ^= 1;
+        const int xk = (int)(key & 1ull);
+        const double gprev = gk;  // gain of k before the flip (exact for int / float64 fields)
+        // float32 fields rank the candidates; the float64 gain of k, summed over
+        // row k in the same pass, decides: not positive -> a second pass undoes
+        // the flip and the ascent stops (one call site for both passes)
+        bool undone = false;
+#pragma unroll 1
+        for (int pass = 0; pass < 2; ++pass) {
+          flip_and_select<WT, GT, CH, STG, BT>(c, k, xk ^ pass, red_key, red_g, red_x, par, &key, &gk, &gx);
+          par ^= 1;
+          if (pass == 1 || !F32 || gx > 0.0) {
+            undone = pass == 1;
+            break;
+          }
+        }
+        if (undone) break;
+        val += scale * (F32 ? gx : gprev);
         ++nflips;
       }
       if (val > best) {
@@ -440,9 +487,9 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
         const double gp = xp ? (double)c.g[fpos<BT>(pick)] : -(double)c.g[fpos<BT>(pick)];
         __syncthreads();  // everyone has read bit, field and kicked set before they change
         if (threadIdx.x == 0) kicked[pick >> 5] |= 1u << (pick & 31);
-        val += scale * gp;
-        flip_and_select<WT, GT, CH, STG, BT>(c, pick, xp, red_key, red_g, par, &key, &gk);
+        flip_and_select<WT, GT, CH, STG, BT>(c, pick, xp, red_key, red_g, red_x, par, &key, &gk, &gx);
         par ^= 1;
+        val += scale * (F32 ? gx : gp);  // float64 gain of the kicked node
         ++nflips;
       }
     }

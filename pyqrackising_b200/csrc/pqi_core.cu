@@ -248,86 +248,151 @@ __global__ void select_finish_kernel(const unsigned long long* key, SelGeom geo,
 }
 
 // ---------------------------------------------------------------------------
-// Double flips: each block takes rows k and n - 2 - k together (n pair values
-// per block, whatever k), threads over l > k. The pair value is read from the
-// maintained gains: flipping k and l gains g_k + g_l - 2 x_k x_l W_kl.
+// Double flips (kernels.cl:150-231 semantics, from maintained gains).
 //
-// The selection key of pair index i (sel_key) needs i mod G and i / G, and the
-// slot's tie rank. TAB: both are carried incrementally along a thread's l
-// sequence (i advances by the block size each step), and a table in shared
-// memory maps the slot t = i mod G to (group * L + rank) * J (or "never wins"),
-// so the inner loop has no division. Pair indices are below G * J < 2^32.
+// Flipping k and l gains d = g_k + g_l - 2 x_k x_l W_kl; the reference's value
+// is float(d) (x2 for a spin glass) and its selection is the maximum 64-bit
+// key (sel_key) over all pairs k < l in k-major order.
+//
+// The upper triangle is cut into tiles of DR rows x (VEC x 256) columns, each
+// W element read once (16-byte loads, VEC consecutive columns per thread);
+// a thread keeps its columns' gains and bits in registers across the tile's
+// rows. Every pair first gets an fp32 estimate a = (f_k + f_l) + c W_kl
+// (f = float(g), c = -2 when the bits agree, else +2). |a - value| is below
+// 2^-22 (|g_k| + |g_l| + |a|), so a pair with a < thr - delta,
+// delta = 2^-20 (max|g_k| + max|g_l| + |thr|), has value < thr; thr is a value
+// some selectable pair (key != 0) reaches, so such a pair cannot be the
+// maximum and is skipped. Only the remaining pairs - the first ones a thread
+// meets, then the rare near-maxima - take the exact float64 value and key.
+// thr is shared per block (shared memory) and across blocks (one global
+// word), both as order-preserving uint32 under atomicMax.
 
-constexpr int kDoubleTab = 2048;  // slots the table holds; a larger G takes the direct key
+constexpr int DR = 8;                 // rows per tile
+constexpr int DTHREADS = 256;
 
-template <typename WT, bool TAB>
-__global__ void __launch_bounds__(256) double_kernel(const WT* __restrict__ Wp, int ld, int n,
-                              const uint32_t* __restrict__ theta, const double* __restrict__ g64,
-                              int spin, SelGeom geo, unsigned long long* key) {
+template <typename WT>
+struct DoubleVec {
+  static constexpr int VEC = sizeof(WT) == 4 ? 4 : 16;  // columns per thread (16 bytes)
+};
+
+__device__ __forceinline__ float thr_of(uint32_t o) {
+  // ordered 0 (nothing published yet) and anything below -inf read as -inf
+  return o < ord_f32(-INFINITY) ? -INFINITY : unord_f32(o);
+}
+
+template <typename WT>
+__global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
+    const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
+    const double* __restrict__ g64, int spin, SelGeom geo, unsigned long long* key,
+    unsigned int* gthr) {
+  constexpr int VEC = DoubleVec<WT>::VEC;
+  constexpr int CW = VEC * DTHREADS;  // columns per tile
+  constexpr int BAND = CW / DR;       // row groups sharing one first column chunk
   __shared__ uint64_t scratch[32];
-  __shared__ uint32_t tab[TAB ? kDoubleTab : 1];
-  if constexpr (TAB) {
-    for (uint32_t t = threadIdx.x; t < geo.G; t += blockDim.x) {
-      const uint32_t grp = t / geo.L;
-      const uint32_t r = geo.rank[t - grp * geo.L];
-      tab[t] = (r == 0xFFu) ? 0xFFFFFFFFu : (grp * geo.L + r) * geo.J;
-    }
-  }
+  __shared__ unsigned int s_thr;
+  if (threadIdx.x == 0) s_thr = 0u;
   __syncthreads();
-  const uint32_t step_t = blockDim.x % geo.G, step_j = blockDim.x / geo.G;
+  const int ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
+  const int nc = (n + CW - 1) / CW;      // column chunks
+  const int nbands = (ng + BAND - 1) / BAND;
+  long long total = 0;
+  for (int b = 0; b < nbands; ++b)
+    total += (long long)(min(ng, (b + 1) * BAND) - b * BAND) * (nc - b);
   uint64_t best = 0;
-  const int half = n >> 1;  // row pairs (p, n - 2 - p), p < half; one row when they meet
-  for (int p = blockIdx.x; p < half; p += gridDim.x) {
-    for (int side = 0; side < 2; ++side) {
-      const int k = side ? n - 2 - p : p;
-      if (side && k == p) continue;
-      const double gk = g64[k];
-      const int xk = get_bit32(theta, k);
-      const uint32_t base = (uint32_t)(pair_base(k, n) - (k + 1));  // pair (k, l) = base + l
-      const WT* row = Wp + (size_t)k * ld;
-      int l = k + 1 + threadIdx.x;
-      uint32_t i = base + (uint32_t)l;
-      uint32_t t = i % geo.G, j = i / geo.G;
-      // one pair: value from the gains, then its selection key
-      auto pair = [&](WT wr, double gl, uint32_t word, int ll) {
-        const double w = (double)wr;
-        const double d = gk + gl - ((((word >> (ll & 31)) & 1u) == (uint32_t)xk) ? 2.0 * w : -2.0 * w);
-        float v = (float)d;
-        if (spin) v *= 2.0f;
-        uint64_t kk;
-        if constexpr (TAB) {
-          const uint32_t pr = tab[t];
-          kk = (pr == 0xFFFFFFFFu || v != v)
-                   ? 0ull
-                   : (((uint64_t)ord_f32(v) << 32) | (uint64_t)(0xFFFFFFFFu - (pr + j)));
-        } else {
-          kk = sel_key(v, (uint64_t)i, geo);
-        }
-        best = kk > best ? kk : best;
-        i += blockDim.x;
-        t += step_t;
-        j += step_j;
-        if (t >= geo.G) {
-          t -= geo.G;
-          ++j;
-        }
-      };
-      // four steps' loads in flight before any is used
-      const int bd = blockDim.x;
-      for (; l + 3 * bd < n; l += 4 * bd) {
-        WT wr[4];
-        double gl[4];
-        uint32_t wd[4];
+  float thr = -INFINITY;
+  for (long long tau = blockIdx.x; tau < total; tau += gridDim.x) {
+    // tile tau -> (row group rg, column chunk c): band b holds row groups
+    // [b BAND, (b+1) BAND), each with chunks b .. nc-1 (chunks left of b lie
+    // wholly below the diagonal)
+    long long r = tau;
+    int b = 0;
+    while (true) {
+      const long long cnt = (long long)(min(ng, (b + 1) * BAND) - b * BAND) * (nc - b);
+      if (r < cnt) break;
+      r -= cnt;
+      ++b;
+    }
+    const int per = nc - b;
+    const int rg = b * BAND + (int)(r / per);
+    const int c = b + (int)(r - (long long)(r / per) * per);
+    const int k0 = rg * DR;
+    const int l0 = c * CW + threadIdx.x * VEC;
+    // the tile's rows: gains and bits (the same for every thread)
+    float fk[DR];
+    uint32_t xk = 0;
+    float gt = 0.0f;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          wr[u] = row[l + u * bd];
-          gl[u] = __ldg(g64 + l + u * bd);
-          wd[u] = __ldg(theta + ((l + u * bd) >> 5));
-        }
+    for (int i = 0; i < DR; ++i) {
+      const int k = min(k0 + i, n - 1);
+      fk[i] = (float)__ldg(g64 + k);
+      gt = fmaxf(gt, fabsf(fk[i]));
+      xk |= (uint32_t)get_bit32(theta, k) << i;
+    }
+    // this thread's columns
+    float fl[VEC];
+    float cl[VEC];  // -2 where x_l = +1, +2 where x_l = -1
+    float flmax = 0.0f;
+    const uint32_t lw = l0 < n ? __ldg(theta + (l0 >> 5)) >> (l0 & 31) : 0u;
 #pragma unroll
-        for (int u = 0; u < 4; ++u) pair(wr[u], gl[u], wd[u], l + u * bd);
+    for (int e = 0; e < VEC; ++e) {
+      const int l = l0 + e;
+      fl[e] = l < n ? (float)__ldg(g64 + l) : 0.0f;
+      flmax = fmaxf(flmax, fabsf(fl[e]));
+      cl[e] = ((lw >> e) & 1u) ? -2.0f : 2.0f;
+    }
+    // every row's W slice in flight before any is used (l0 < n keeps the
+    // 16-byte load inside the padded row of ld >= n elements)
+    WT w[DR][VEC];
+#pragma unroll
+    for (int i = 0; i < DR; ++i) {
+      const int k = min(k0 + i, n - 1);
+      if (l0 < n) {
+        const int4 v = __ldg(reinterpret_cast<const int4*>(Wp + (size_t)k * ld + l0));
+        memcpy(&w[i][0], &v, 16);
+      } else {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) w[i][e] = (WT)0;
       }
-      for (; l < n; l += bd) pair(row[l], __ldg(g64 + l), __ldg(theta + (l >> 5)), l);
+    }
+    thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(gthr))));
+    const float base = gt + flmax;
+    float cut = thr - ldexpf(base + fabsf(thr), -20);
+#pragma unroll
+    for (int i = 0; i < DR; ++i) {
+      // c = -2 when bits k and l agree: cl already is for x_k = +1; x_k = -1 flips its sign
+      const uint32_t flip = (((xk >> i) & 1u) ^ 1u) << 31;
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) {
+        const float cc = __uint_as_float(__float_as_uint(cl[e]) ^ flip);
+        const float a = fmaf(cc, (float)w[i][e], fk[i] + fl[e]);
+        if (a >= cut) {
+          const int k = k0 + i, l = l0 + e;
+          if (k < n - 1 && l > k && l < n) {
+            const double gk = __ldg(g64 + k), gl = __ldg(g64 + l);
+            const double wd = (double)w[i][e];
+            const bool agree = (((lw >> e) & 1u) == ((xk >> i) & 1u));
+            const double d = gk + gl - (agree ? 2.0 * wd : -2.0 * wd);
+            float v = (float)d;
+            if (spin) v *= 2.0f;
+            const uint64_t kk =
+                sel_key(v, (uint64_t)(pair_base(k, n) + (long long)(l - k - 1)), geo);
+            best = kk > best ? kk : best;
+            const float vu = (float)d;
+            if (kk != 0ull && vu > thr) {
+              thr = vu;
+              cut = thr - ldexpf(base + fabsf(thr), -20);
+            }
+          }
+        }
+      }
+    }
+    // publish this thread's threshold (a value a selectable pair reaches)
+    if (thr > -INFINITY) {
+      const unsigned int o = ord_f32(thr);
+      if (o > *(volatile unsigned int*)&s_thr) {
+        atomicMax(&s_thr, o);
+        if (o > __ldcg(gthr)) atomicMax(gthr, o);
+      }
     }
   }
   best = block_max_u64(best, scratch);
@@ -642,7 +707,7 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
   SelGeom geo;
   PQI_CHECK_ARG(make_sel_geom(combo, global_size, local_size, &geo));
   Workspace ws(workspace, workspace_bytes);
-  unsigned long long* key = ws.take<unsigned long long>(1);
+  unsigned long long* key = ws.take<unsigned long long>(2);  // key, then the threshold word
   PQI_CHECK_ARG(key);
   cudaStream_t s = as_stream(stream);
   if (!gains64) {
@@ -652,37 +717,28 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     if (rc) return rc;
     gains64 = g;
   }
-  PQI_TRY(cudaMemsetAsync(key, 0, sizeof(unsigned long long), s));
-  // one resident wave of blocks (a partial second wave would idle most SMs)
-  static int resident[2][2] = {{0, 0}, {0, 0}};
-  const bool tab = geo.G <= (uint32_t)kDoubleTab;
+  // key (8 bytes) and the shared threshold (4 bytes), zeroed together
+  PQI_TRY(cudaMemsetAsync(key, 0, 16, s));
+  unsigned int* gthr = reinterpret_cast<unsigned int*>(key + 1);
+  // one resident wave of blocks, persistent over the tiles
+  static int resident[2] = {0, 0};
   const int i8 = w->kind == PQI_W_I8 ? 1 : 0;
-  if (!resident[i8][tab]) {
+  if (!resident[i8]) {
     int dev = 0, sms = 0, per_sm = 0;
     PQI_TRY(cudaGetDevice(&dev));
     PQI_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const void* fn = i8 ? (tab ? (const void*)double_kernel<int8_t, true> : (const void*)double_kernel<int8_t, false>)
-                        : (tab ? (const void*)double_kernel<float, true> : (const void*)double_kernel<float, false>);
-    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
-    resident[i8][tab] = std::max(1, sms * std::max(1, per_sm));
+    const void* fn = i8 ? (const void*)double_tile_kernel<int8_t> : (const void*)double_tile_kernel<float>;
+    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, DTHREADS, 0));
+    resident[i8] = std::max(1, sms * std::max(1, per_sm));
   }
-  const int grid = std::max(1, std::min(n >> 1, resident[i8][tab]));
-  if (w->kind == PQI_W_I8) {
-    if (tab)
-      double_kernel<int8_t, true><<<grid, 256, 0, s>>>(w->W_i8, w->ld, n, theta, gains64,
-                                                       is_spin_glass, geo, key);
-    else
-      double_kernel<int8_t, false><<<grid, 256, 0, s>>>(w->W_i8, w->ld, n, theta, gains64,
-                                                        is_spin_glass, geo, key);
+  if (i8) {
+    double_tile_kernel<int8_t><<<resident[i8], DTHREADS, 0, s>>>(w->W_i8, w->ld, n, theta, gains64,
+                                                                is_spin_glass, geo, key, gthr);
   } else {
-    if (tab)
-      double_kernel<float, true><<<grid, 256, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64,
-                                                      is_spin_glass, geo, key);
-    else
-      double_kernel<float, false><<<grid, 256, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64,
-                                                       is_spin_glass, geo, key);
+    double_tile_kernel<float><<<resident[i8], DTHREADS, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64,
+                                                               is_spin_glass, geo, key, gthr);
   }
-  PQI_LAUNCHED("double_kernel");
+  PQI_LAUNCHED("double_tile_kernel");
   select_finish_kernel<<<1, 1, 0, s>>>(key, geo, best_energy, best_index);
   PQI_LAUNCHED("select_finish_kernel");
   return PQI_OK;

@@ -198,12 +198,20 @@ __global__ void __launch_bounds__(1024) descent_kernel(
   double esum = 0.0;
   int cnt = 0, st = PQI_OK;
   while (true) {
+    // a value below the thread's best so far cannot give a larger key: the
+    // key (and its divisions) only for candidates that reach it
     uint64_t best = 0;
+    float bv = -INFINITY;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
       float v = (float)g[k];
       if (spin) v *= 2.0f;
-      const uint64_t kk = sel_key(v, (uint64_t)k, geo);
-      best = kk > best ? kk : best;
+      if (v >= bv) {
+        const uint64_t kk = sel_key(v, (uint64_t)k, geo);
+        if (kk > best) {
+          best = kk;
+          bv = v;
+        }
+      }
     }
     best = block_max_u64(best, scratch);
     float val;

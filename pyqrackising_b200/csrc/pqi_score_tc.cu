@@ -66,11 +66,20 @@ constexpr uint32_t kIdescBF16 = (1u << 4)    // D: f32
 constexpr uint32_t kIdescI8Pair = (kIdescI8 & ~(0x1Fu << 24)) | ((uint32_t)(256 >> 4) << 24);
 constexpr uint32_t kIdescBF16Pair = (kIdescBF16 & ~(0x1Fu << 24)) | ((uint32_t)(256 >> 4) << 24);
 
-// Warp roles of the persistent kernel (6 warps).
-constexpr int TMA_WARP = 0;       // warp 0 lane 0: TMA loads of the X and W tiles
+// Warp roles of the persistent kernel (6 warps, 10 when the A operand is
+// expanded in the kernel).
+constexpr int TMA_WARP = 0;       // warp 0 lane 0: TMA loads of the W (and X) tiles
 constexpr int MMA_WARP = 1;       // warp 1: TMEM alloc, lane 0 issues MMAs
 constexpr int PTHREADS = 192;     // warps 2-5: epilogue (TMEM lane quarter = warp % 4)
+constexpr int FTHREADS = 320;     // + warps 6-9: A-operand producers (FUSED)
 constexpr int ACC_COLS = 512;     // two 256-column accumulators
+// FUSED: each producer thread owns one A row; the packed bits it needs run
+// PF stages ahead through a per-thread cp.async ring in shared memory
+// (16 bytes per stage: four words of int8 columns, two of bf16 columns).
+constexpr int PF = 6;
+constexpr int PF_BYTES = PF * 128 * 16;  // 12 KB
+constexpr int SMEM_BYTES_FUSED = STAGES * STAGE_BYTES + PF_BYTES + 1024;
+static_assert(SMEM_BYTES_FUSED <= 227 * 1024, "fused ring fits");
 
 __device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 
@@ -81,8 +90,36 @@ __device__ __forceinline__ void epi_barrier() { asm volatile("bar.sync 1, 128;" 
 // split between two CTAs goes through per-tile partials summed in tile order
 // by the CTA that completes it. The finisher converts q to the reference's
 // value and folds it into the selection key; the last block decodes it.
-template <bool kInt8, bool PAIR>
-__global__ void __launch_bounds__(PTHREADS, 1)
+// One packed word (32 columns) of a candidate -> the A operand's 16-byte
+// chunks: int8 +-1 (32 bytes = two chunks) or bf16 +-1 (64 bytes = four
+// chunks); bit set = +1.
+__device__ __forceinline__ void pm1_i8x4(uint32_t nib, uint32_t& o) {
+  // four bits -> four bytes 0x01 (set) / 0xFF (clear)
+  const uint32_t t = ((nib & 0xFu) * 0x00204081u) & 0x01010101u;
+  o = 0xFFFFFFFFu - t * 0xFEu;
+}
+
+__device__ __forceinline__ uint32_t pm1_bf16x2(uint32_t two) {
+  // two bits -> two bf16: 0x3F80 (+1) / 0xBF80 (-1)
+  const uint32_t nb = ~two;
+  return 0x3F803F80u | ((nb & 1u) << 15) | ((nb & 2u) << 30);
+}
+
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src),
+               "r"(valid ? 4 : 0)
+               : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <bool kInt8, bool PAIR, bool FUSED>
+__global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
     score_tc_kernel(const __grid_constant__ CUtensorMap map_a,
                     const __grid_constant__ CUtensorMap map_b0,
                     const __grid_constant__ CUtensorMap map_b1, int n, int shots,
@@ -125,7 +162,8 @@ __global__ void __launch_bounds__(PTHREADS, 1)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NST; ++s) {
-      mbar_init(&full_bar[s], 1);
+      // FUSED: the W tile's TMA arrival plus one arrival per producer warp
+      mbar_init(&full_bar[s], FUSED ? 5 : 1);
       mbar_init(&empty_bar[s], 1);
     }
     for (int a = 0; a < 2; ++a) {
@@ -181,6 +219,9 @@ __global__ void __launch_bounds__(PTHREADS, 1)
             const uint32_t bar = smem_u32(&full_bar[s]) & kPeerMask;
             tma_load_2d_pair(dst, &map_a, bar, kk, m0);
             tma_load_2d_pair(dst + A_STAGE, mb, bar, kk, n0);
+          } else if constexpr (FUSED) {
+            mbar_expect_tx(&full_bar[s], B_STAGE);  // the producers write the A tile
+            tma_load_2d(dst + A_STAGE, mb, &full_bar[s], kk, n0);
           } else {
             mbar_expect_tx(&full_bar[s], STAGE_BYTES);
             tma_load_2d(dst, &map_a, &full_bar[s], kk, m0);
@@ -242,6 +283,71 @@ __global__ void __launch_bounds__(PTHREADS, 1)
       if (!ok) s_fail = 1;
     }
     __syncwarp();
+  } else if (FUSED && warp >= 6) {
+    // ---- A producers: warps 6-9, thread p writes row p of every A tile ----
+    // Stage it of this CTA is tile t_begin + it / kblocks, K block
+    // it % kblocks. The row's packed words for stage it + PF are copied into
+    // the thread's ring slot while stage it is expanded, so the L2 latency of
+    // the bits is hidden behind PF stages of MMAs.
+    const int p = threadIdx.x - 192;
+    constexpr int WPS = kInt8 ? 4 : 2;  // packed words per stage
+    const long long nstage = (long long)(t_end - t_begin) * kblocks;
+    const uint32_t ring = smem_u32(smem + NST * SB) + (uint32_t)p * 16u;
+    auto issue = [&](long long st) {
+      if (st < nstage) {
+        const int t = t_begin + (int)(st / kblocks), kb = (int)(st % kblocks);
+        const int b = (t / ntn) * BM + p;
+        const int w0 = kInt8 ? kb * 4 : (kb % kb_per_pass) * 2;
+        const uint32_t* src = theta + (size_t)(b < shots ? b : 0) * n32;
+        const uint32_t dst = ring + (uint32_t)((st % PF) * 128 * 16);
+#pragma unroll
+        for (int q = 0; q < WPS; ++q)
+          cp_async4(dst + 4 * q, src + min(w0 + q, n32 - 1), b < shots && w0 + q < n32);
+      }
+      cp_async_commit();  // an empty group past the end keeps the count uniform
+    };
+#pragma unroll 1
+    for (int q = 0; q < PF; ++q) issue(q);
+    bool ok = true;
+#pragma unroll 1
+    for (long long st = 0; st < nstage; ++st) {
+      cp_async_wait<PF - 1>();  // this stage's words have landed
+      uint32_t wd[4];
+      const uint8_t* slot = smem + NST * SB + (size_t)p * 16 + (size_t)(st % PF) * 128 * 16;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) wd[q] = (q < WPS) ? *reinterpret_cast<const volatile uint32_t*>(slot + 4 * q) : 0u;
+      issue(st + PF);
+      const int s = (int)(st % NST);
+      if (st >= NST && !mbar_wait(&empty_bar[s], (uint32_t)((st / NST) - 1) & 1u)) {
+        ok = false;
+        s_fail = 1;
+      }
+      if (__all_sync(0xFFFFFFFFu, ok)) {
+        // row p of the 128-byte-swizzled K-major tile: 16-byte chunk c sits at
+        // (c ^ (p & 7)) * 16 in the row
+        uint8_t* rowp = smem + s * SB + p * BK_BYTES;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          uint32_t o[4];
+          if constexpr (kInt8) {
+            const uint32_t bits16 = (wd[c >> 1] >> ((c & 1) * 16)) & 0xFFFFu;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) pm1_i8x4(bits16 >> (4 * e), o[e]);
+          } else {
+            const uint32_t bits8 = (wd[c >> 2] >> ((c & 3) * 8)) & 0xFFu;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) o[e] = pm1_bf16x2(bits8 >> (2 * e));
+          }
+          *reinterpret_cast<uint4*>(rowp + ((c ^ (p & 7)) << 4)) = make_uint4(o[0], o[1], o[2], o[3]);
+        }
+        // generic-proxy writes -> visible to the tensor core (async proxy)
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      }
+      __syncwarp();
+      if (!__all_sync(0xFFFFFFFFu, ok)) break;
+      if (lane == 0) mbar_arrive(&full_bar[s]);
+    }
+    cp_async_wait<0>();
   } else {
     // ---- epilogue: warps 2-5, all 128 threads take every branch together ----
     const int quarter = warp & 3;
@@ -569,13 +675,19 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
   if (i8 && n > 65536) return PQI_ENOTSUP;
   const int ntn = (n + tc::BN - 1) / tc::BN;
   const int ntm = (shots + tc::BM - 1) / tc::BM;
+  // 0 (default): single CTAs that expand the packed candidates into the A
+  // tiles themselves; 2: single CTAs, A expanded by a separate pass and loaded
+  // by TMA; 3: CTA pairs (cta_group::2), A as in 2
+  const bool fused = g_score_path == 0;
+  const bool pair = g_score_path == 3 && ntm >= 2;
   // one zeroed control block: err, mdone, key, then mcount[ntm]
   const size_t ctl_bytes = 64 + (size_t)ntm * sizeof(unsigned);
   uint8_t* ctl = ws.take<uint8_t>(ctl_bytes);
   double* qpart = ws.take<double>((size_t)ntn * shots);
-  void* X = i8 ? (void*)ws.take<int8_t>((size_t)shots * ld)
-               : (void*)ws.take<uint16_t>((size_t)shots * ld);
-  if (!ctl || !qpart || !X) return PQI_EINVAL;
+  void* X = nullptr;
+  if (!fused)
+    X = i8 ? (void*)ws.take<int8_t>((size_t)shots * ld) : (void*)ws.take<uint16_t>((size_t)shots * ld);
+  if (!ctl || !qpart || (!fused && !X)) return PQI_EINVAL;
   int* err = reinterpret_cast<int*>(ctl);
   unsigned* mdone = reinterpret_cast<unsigned*>(ctl + 8);
   unsigned long long* key = reinterpret_cast<unsigned long long*>(ctl + 16);
@@ -585,34 +697,41 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
   } else if (!w->W_hi || !w->W_lo) {
     return PQI_EINVAL;
   }
-  // CTA pairs (cta_group::2) for batches of more than one 128-candidate block,
-  // unless the single-CTA form is selected (pqi_score_set_path(2))
-  const bool pair = ntm >= 2 && g_score_path != 2;
   const int brows = pair ? tc::BN / 2 : tc::BN;
   CUtensorMap ma, mb0, mb1;
-  if (!cached_map(&ma, X, i8, shots, n, ld, tc::BM)) return PQI_ENOTSUP;
   if (!cached_map(&mb0, i8 ? (const void*)w->W_i8 : (const void*)w->W_hi, i8, n, n, ld, brows))
     return PQI_ENOTSUP;
   if (!cached_map(&mb1, i8 ? (const void*)w->W_i8 : (const void*)w->W_lo, i8, n, n, ld, brows))
     return PQI_ENOTSUP;
-  static bool attr_set[2][2] = {{false, false}, {false, false}};
-  if (!attr_set[i8][pair]) {
-    const void* k = i8 ? (pair ? (const void*)tc::score_tc_kernel<true, true>
-                               : (const void*)tc::score_tc_kernel<true, false>)
-                       : (pair ? (const void*)tc::score_tc_kernel<false, true>
-                               : (const void*)tc::score_tc_kernel<false, false>);
-    PQI_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::SMEM_BYTES));
-    attr_set[i8][pair] = true;
+  if (fused) {
+    ma = mb0;  // not read: the kernel writes its A tiles itself
+  } else if (!cached_map(&ma, X, i8, shots, n, ld, tc::BM)) {
+    return PQI_ENOTSUP;
+  }
+  // kernel instances: [int8][form], form 0 = fused, 1 = single CTA, 2 = pair
+  const int form = fused ? 0 : (pair ? 2 : 1);
+  static const void* const kfn[2][3] = {
+      {(const void*)tc::score_tc_kernel<false, false, true>, (const void*)tc::score_tc_kernel<false, false, false>,
+       (const void*)tc::score_tc_kernel<false, true, false>},
+      {(const void*)tc::score_tc_kernel<true, false, true>, (const void*)tc::score_tc_kernel<true, false, false>,
+       (const void*)tc::score_tc_kernel<true, true, false>}};
+  const int smem_bytes = fused ? tc::SMEM_BYTES_FUSED : tc::SMEM_BYTES;
+  static bool attr_set[2][3] = {};
+  if (!attr_set[i8][form]) {
+    PQI_TRY(cudaFuncSetAttribute(kfn[i8][form], cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes));
+    attr_set[i8][form] = true;
   }
   PQI_TRY(cudaMemsetAsync(ctl, 0, ctl_bytes, s));
-  const long long words = (long long)shots * n32;
-  const int eg = (int)std::max<long long>(1, std::min<long long>((words + 255) / 256, 148 * 16));
-  if (i8) {
-    tc::expand_pm1_kernel<int8_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (int8_t*)X);
-  } else {
-    tc::expand_pm1_kernel<uint16_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (uint16_t*)X);
+  if (!fused) {
+    const long long words = (long long)shots * n32;
+    const int eg = (int)std::max<long long>(1, std::min<long long>((words + 255) / 256, 148 * 16));
+    if (i8) {
+      tc::expand_pm1_kernel<int8_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (int8_t*)X);
+    } else {
+      tc::expand_pm1_kernel<uint16_t><<<eg, 256, 0, s>>>(theta, shots, n32, ld, (uint16_t*)X);
+    }
+    PQI_LAUNCHED("expand_pm1_kernel");
   }
-  PQI_LAUNCHED("expand_pm1_kernel");
   const int limit = g_score_grid > 0 ? g_score_grid : num_sms;
   if (g_score_ev_before) PQI_TRY(cudaEventRecord(g_score_ev_before, s));
   if (pair) {
@@ -634,32 +753,33 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     if (!fit[i8]) {
       cfg.gridDim = dim3(2);
       int f = 0;
-      PQI_TRY(cudaOccupancyMaxActiveClusters(
-          &f, i8 ? (const void*)tc::score_tc_kernel<true, true> : (const void*)tc::score_tc_kernel<false, true>,
-          &cfg));
+      PQI_TRY(cudaOccupancyMaxActiveClusters(&f, kfn[i8][2], &cfg));
       fit[i8] = std::max(1, f);
     }
     const int pairs = std::max(1, std::min({tiles, limit / 2, fit[i8]}));
     cfg.gridDim = dim3(2 * pairs);
     if (i8) {
-      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<true, true>, ma, mb0, mb1, n, shots,
+      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<true, true, false>, ma, mb0, mb1, n, shots,
                                  theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
                                  mdone, key, best_energy, best_index, err));
     } else {
-      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<false, true>, ma, mb0, mb1, n, shots,
+      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<false, true, false>, ma, mb0, mb1, n, shots,
                                  theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
                                  mdone, key, best_energy, best_index, err));
     }
   } else {
     const int grid = std::min(ntn * ntm, limit);
+    const int threads = fused ? tc::FTHREADS : tc::PTHREADS;
     if (i8) {
-      tc::score_tc_kernel<true, false><<<grid, tc::PTHREADS, tc::SMEM_BYTES, s>>>(
-          ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
-          mdone, key, best_energy, best_index, err);
+      auto k = fused ? tc::score_tc_kernel<true, false, true> : tc::score_tc_kernel<true, false, false>;
+      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo,
+                                          qpart, energies, mcount, mdone, key, best_energy, best_index,
+                                          err);
     } else {
-      tc::score_tc_kernel<false, false><<<grid, tc::PTHREADS, tc::SMEM_BYTES, s>>>(
-          ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
-          mdone, key, best_energy, best_index, err);
+      auto k = fused ? tc::score_tc_kernel<false, false, true> : tc::score_tc_kernel<false, false, false>;
+      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo,
+                                          qpart, energies, mcount, mdone, key, best_energy, best_index,
+                                          err);
     }
   }
   PQI_LAUNCHED("score_tc_kernel");
