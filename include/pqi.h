@@ -118,9 +118,10 @@ pqi_status pqi_prepare_weights(const float* W, int n, const pqi_weight_stats* st
                                pqi_weights* out_host, void* stream);
 
 /* Select the batched-scoring implementation: 0 = tensor cores (tcgen05, the
- * default; CTA pairs with cta_group::2 MMAs for batches of more than 128
- * candidates), 1 = CUDA cores, 2 = tensor cores with single-CTA MMAs.
- * Process-wide; used to cross-check the implementations. */
+ * default; the kernel expands the packed candidates into its +-1 operand
+ * tiles itself), 1 = CUDA cores, 2 = tensor cores fed by a separate expansion
+ * pass, 3 = as 2 with CTA pairs (cta_group::2 MMAs) for batches of more than
+ * 128 candidates. Process-wide; used to cross-check the implementations. */
 pqi_status pqi_score_set_path(int path);
 
 /* Record two caller-owned cudaEvent_t on the call's stream immediately before
@@ -204,6 +205,9 @@ pqi_status pqi_single_bit_flips(const pqi_weights* w, const uint32_t* theta, int
  * array's device address (cudaGetSymbolAddress, with the device current); make
  * it before any stream capture. All calls share the array, which keeps the last
  * call's contents: calls that overlap on the GPU race. Allocates nothing.
+ * The looked-up address is kept per device ordinal for the life of the
+ * process, so this call serves the device's primary context (the runtime
+ * API's) and must not be used after cudaDeviceReset on that device.
  * Returns PQI_EINVAL when n > PQI_NOALLOC_MAX_N (pqi_last_error() says so).
  * Same outputs as pqi_single_bit_flips.
  */
@@ -418,6 +422,14 @@ pqi_status pqi_mpnn_norm_adj(const float* W, int n, void* Ahat, int ld, float* s
 pqi_status pqi_mpnn_features(const uint32_t* theta, const double* gains64, const float* s,
                              float mean_s, int n, void* F, void* stream);
 
+/* Kick distributions of `tasks` states from their logits (tasks x n,
+ * contiguous): softmax(logit / temperature) in float64, mixed with the
+ * uniform distribution ((1 - mix) p + mix / n), as normalised cumulative
+ * arrays (tasks x n float64, the batched search's kick_cdf). A task with a
+ * non-finite logit gets the uniform distribution. */
+pqi_status pqi_mpnn_kick_cdf(const float* logits, int n, int tasks, float temperature, float mix,
+                             double* cdf, void* stream);
+
 /* Softmax of n logits: *loss = -sum_v t_v log p_v, dlogits = p - t, prob = p
  * (each output and target nullable). One block. */
 pqi_status pqi_mpnn_softmax_xent(const float* logits, const float* target, int n, float* loss,
@@ -542,6 +554,87 @@ pqi_status pqi_pack_bits(const uint8_t* bools, int rows, int n, uint32_t* words,
 
 /* words (rows x ceil(n/32)) -> bytes 0/1 (rows x n). */
 pqi_status pqi_unpack_bits(const uint32_t* words, int rows, int n, uint8_t* bools, void* stream);
+
+/* ---------------------------------------------------------------------------
+ * Sparse graphs: the coupling matrix in compressed rows (CSR), O(n + nnz)
+ * device memory, for graphs too large to hold as an n x n matrix. Replaces
+ * the reference's CSR kernels (kernels.cl:233-414, 1072-1150) and buffers
+ * (make_G_m_csr_buf, spin_glass_solver_sparse.py:659-661). Every entry point
+ * has the semantics of its dense counterpart above (same values, same
+ * reference-order selection); a flip costs O(degree).
+ * -------------------------------------------------------------------------*/
+
+/* Both triangles stored: row r lists every neighbour c != r once, columns
+ * ascending, with val = W_rc = W_cr. ptr has n + 1 entries (ptr[0] = 0,
+ * ptr[n] = nnz). */
+typedef struct {
+  const long long* ptr;
+  const int* col;
+  const float* val;
+  int n;
+  int pad;
+  long long nnz;
+  double upper_sum; /* sum over edges u < v of W_uv (float64, host value) */
+} pqi_csr;
+
+/* Gains of `count` states (rows of ceil(n/32) words): g_k = sum over
+ * neighbours v of W_kv (s_k == s_v ? +1 : -1), float64 (and/or float32).
+ * Replaces the sums of single_bit_flips_sparse (kernels.cl:253-283). */
+pqi_status pqi_csr_gains(const pqi_csr* g, const uint32_t* theta, int count, float* g32,
+                         double* g64, void* stream);
+
+/* pqi_single_bit_flips on CSR (kernels.cl:233-283 with the host argmax). */
+pqi_status pqi_csr_single_bit_flips(const pqi_csr* g, const uint32_t* theta, int is_spin_glass,
+                                    int global_size, int local_size, float* best_energy,
+                                    int* best_index, void* workspace, size_t workspace_bytes,
+                                    void* stream);
+
+/* pqi_apply_flip on CSR: O(degree) per flipped node. */
+pqi_status pqi_csr_apply_flip(const pqi_csr* g, uint32_t* theta, double* gains64, int k, int l,
+                              void* stream);
+
+/* pqi_single_descent on CSR (one CTA; gains updated in place in gains64).
+ * Synchronises `stream`; returns PQI_ETIMEOUT when max_flips runs out. */
+pqi_status pqi_csr_single_descent(const pqi_csr* g, uint32_t* theta, double* gains64,
+                                  int is_spin_glass, int global_size, int local_size,
+                                  int max_flips, double* energy_sum, int* flips, int* trace,
+                                  void* workspace, size_t workspace_bytes, void* stream);
+
+/* pqi_double_bit_flips on CSR over all n(n-1)/2 pairs (kernels.cl:285-414
+ * semantics): the pair index c = k(n-1) - k(k-1)/2 + (l-k-1) is 64-bit
+ * (best_index), so n above 46341, where the reference's int32 pair count
+ * overflows, has a defined result (the same rule with 64-bit indices).
+ * gains64 nullable (computed here when NULL). */
+pqi_status pqi_csr_double_bit_flips(const pqi_csr* g, const uint32_t* theta, const double* gains64,
+                                    int is_spin_glass, int global_size, int local_size,
+                                    float* best_energy, long long* best_index, void* workspace,
+                                    size_t workspace_bytes, void* stream);
+
+/* pqi_gray on CSR (the gray_sparse kernel's schedule, kernels.cl:1072-1150);
+ * gains64 required. Workspace: n float64 per resident seed. */
+pqi_status pqi_csr_gray(const pqi_csr* g, const uint64_t* theta64, const double* gains64,
+                        int is_spin_glass, long long iters_bound, int seeds, uint64_t* theta_out,
+                        float* energy_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* float64 cut and energy of `rows` states (compute_cut_sparse /
+ * compute_energy_sparse, maxcut_tfim_util.py:349-372, on the symmetric rows). */
+pqi_status pqi_csr_rescore_fp64(const pqi_csr* g, const uint32_t* words, int rows, double* cut,
+                                double* energy, void* stream);
+
+/* The TFIM sampler's J_eff and degrees from the stored rows S (CSR as the
+ * caller stores them, columns ascending; the entries absent from a row are
+ * zeros) with the reference's sparse-path arithmetic (maxcut_tfim_sparse.py:
+ * 204-224; pqi_tfim_jz_f32 on the dense S gives the same values). gmin =
+ * min over all of S, zeros included. */
+pqi_status pqi_csr_tfim_jz(const long long* ptr, const int* col, const float* val, int n, float gmin,
+                           double* J_eff, unsigned int* degrees, void* stream);
+
+/* pqi_calculate_cut on CSR (calculate_cut_sparse semantics): values of `shots`
+ * candidates, O(nnz) each, then the reference-order selection. */
+pqi_status pqi_csr_calculate_cut(const pqi_csr* g, const uint32_t* theta, int shots,
+                                 int is_spin_glass, int global_size, int local_size,
+                                 float* energies, float* best_energy, int* best_index,
+                                 void* workspace, size_t workspace_bytes, void* stream);
 
 #ifdef __cplusplus
 }

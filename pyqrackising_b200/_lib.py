@@ -65,11 +65,26 @@ class PqiWeightStats(ctypes.Structure):
     ]
 
 
+class PqiCsr(ctypes.Structure):
+    """Mirror of ``pqi_csr`` (include/pqi.h)."""
+
+    _fields_ = [
+        ("ptr", ctypes.c_void_p),
+        ("col", ctypes.c_void_p),
+        ("val", ctypes.c_void_p),
+        ("n", ctypes.c_int),
+        ("pad", ctypes.c_int),
+        ("nnz", ctypes.c_longlong),
+        ("upper_sum", ctypes.c_double),
+    ]
+
+
 _vp = ctypes.c_void_p
 _i = ctypes.c_int
 _l = ctypes.c_long
 _sz = ctypes.c_size_t
 _WP = ctypes.POINTER(PqiWeights)
+_CP = ctypes.POINTER(PqiCsr)
 
 # name -> (restype, argtypes); every function of include/pqi.h
 SIGNATURES = {
@@ -105,6 +120,7 @@ SIGNATURES = {
     "pqi_mpnn_norm_adj": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
     "pqi_mpnn_features": (_i, [_vp, _vp, _vp, ctypes.c_float, _i, _vp, _vp]),
     "pqi_mpnn_softmax_xent": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp]),
+    "pqi_mpnn_kick_cdf": (_i, [_vp, _i, _i, ctypes.c_float, ctypes.c_float, _vp, _vp]),
     "pqi_mpnn_relu_bwd": (_i, [_vp, _vp, _sz, _vp, _vp, _vp]),
     "pqi_mpnn_colsum": (_i, [_vp, _i, _i, _i, _vp, _i, _vp]),
     "pqi_mpnn_to_bf16": (_i, [_vp, _sz, _vp, _vp]),
@@ -125,6 +141,15 @@ SIGNATURES = {
     "pqi_rescore_fp64": (_i, [_WP, _vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_pack_bits": (_i, [_vp, _i, _i, _vp, _vp]),
     "pqi_unpack_bits": (_i, [_vp, _i, _i, _vp, _vp]),
+    "pqi_csr_gains": (_i, [_CP, _vp, _i, _vp, _vp, _vp]),
+    "pqi_csr_single_bit_flips": (_i, [_CP, _vp, _i, _i, _i, _vp, _vp, _vp, _sz, _vp]),
+    "pqi_csr_apply_flip": (_i, [_CP, _vp, _vp, _i, _i, _vp]),
+    "pqi_csr_single_descent": (_i, [_CP, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "pqi_csr_double_bit_flips": (_i, [_CP, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _sz, _vp]),
+    "pqi_csr_gray": (_i, [_CP, _vp, _vp, _i, ctypes.c_longlong, _i, _vp, _vp, _vp, _sz, _vp]),
+    "pqi_csr_rescore_fp64": (_i, [_CP, _vp, _i, _vp, _vp, _vp]),
+    "pqi_csr_calculate_cut": (_i, [_CP, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "pqi_csr_tfim_jz": (_i, [_vp, _vp, _vp, _i, ctypes.c_float, _vp, _vp, _vp]),
 }
 
 _lib = None

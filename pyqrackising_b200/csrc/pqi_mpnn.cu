@@ -237,7 +237,101 @@ static int grid1(size_t work, int block = 256) {
 
 using namespace pqi;
 
+// Kick distribution of each task from its logits (one CTA per task): p =
+// softmax(logit / T) in float64, mixed with the uniform distribution
+// ((1 - mix) p + mix / n), as a normalised cumulative array; any non-finite
+// logit makes the task's distribution uniform (the search must not depend on
+// the network being right).
+__global__ void __launch_bounds__(1024) kick_cdf_kernel(const float* __restrict__ logits, int n,
+                                                        float inv_t, float mix,
+                                                        double* __restrict__ cdf) {
+  __shared__ double sred[32];
+  __shared__ double s_bcast;
+  __shared__ int s_bad;
+  const float* z = logits + (size_t)blockIdx.x * n;
+  double* out = cdf + (size_t)blockIdx.x * n;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) s_bad = 0;
+  __syncthreads();
+  // 1. max of z / T (and a non-finite check)
+  double m = -INFINITY;
+  for (int v = threadIdx.x; v < n; v += blockDim.x) {
+    const float x = z[v];
+    if (!isfinite(x)) s_bad = 1;
+    m = fmax(m, (double)x * (double)inv_t);
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  if (lane == 0) sred[warp] = m;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = -INFINITY;
+    for (int i = 0; i < nw; ++i) t = fmax(t, sred[i]);
+    s_bcast = t;
+  }
+  __syncthreads();
+  const bool uniform = s_bad != 0;
+  const double zmax = s_bcast;
+  __syncthreads();
+  // 2. sum of the unnormalised weights
+  double sum = 0.0;
+  for (int v = threadIdx.x; v < n; v += blockDim.x)
+    sum += uniform ? 1.0 : exp((double)z[v] * (double)inv_t - zmax);
+  for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+  if (lane == 0) sred[warp] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < nw; ++i) t += sred[i];
+    s_bcast = t;
+  }
+  __syncthreads();
+  const double total = s_bcast;
+  __syncthreads();
+  // 3. running sum in chunks of blockDim, warp scans then the warp totals
+  double carry = 0.0;
+  for (int base = 0; base < n; base += blockDim.x) {
+    const int v = base + threadIdx.x;
+    double p = 0.0;
+    if (v < n) {
+      const double w = uniform ? 1.0 : exp((double)z[v] * (double)inv_t - zmax);
+      p = (1.0 - (double)mix) * (w / total) + (double)mix / (double)n;
+    }
+    double x = p;
+    for (int o = 1; o < 32; o <<= 1) {
+      const double y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) sred[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      double t = lane < nw ? sred[lane] : 0.0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xFFFFFFFFu, t, o);
+        if (lane >= o) t += y;
+      }
+      if (lane < nw) sred[lane] = t;  // inclusive prefix of the warp totals
+    }
+    __syncthreads();
+    const double before = carry + (warp > 0 ? sred[warp - 1] : 0.0);
+    if (v < n) out[v] = before + x;
+    carry += sred[nw - 1];
+    __syncthreads();
+  }
+  // 4. normalise by the last entry
+  const double last = out[n - 1];
+  __syncthreads();
+  for (int v = threadIdx.x; v < n; v += blockDim.x) out[v] = out[v] / last;
+}
+
 extern "C" {
+
+pqi_status pqi_mpnn_kick_cdf(const float* logits, int n, int tasks, float temperature, float mix,
+                             double* cdf, void* stream) {
+  PQI_CHECK_ARG(logits && cdf && n > 0 && tasks > 0 && temperature > 0.0f && mix >= 0.0f && mix <= 1.0f);
+  kick_cdf_kernel<<<tasks, 1024, 0, as_stream(stream)>>>(logits, n, 1.0f / temperature, mix, cdf);
+  PQI_LAUNCHED("kick_cdf_kernel");
+  return PQI_OK;
+}
 
 pqi_status pqi_mpnn_gemm(int transA, int transB, int M, int N, int K, float alpha, const void* A,
                          int lda, const void* B, int ldb, float beta, float* C32, void* C16,

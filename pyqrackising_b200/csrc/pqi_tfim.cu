@@ -550,7 +550,8 @@ static pqi_status tfim_sample_impl(const float* W, int n, const double* cum, dou
                                    uint64_t seed, uint64_t round, int shots, uint32_t* theta_out,
                                    void* workspace, size_t workspace_bytes, void* stream,
                                    const long long* adj_ptr, const int* adj_col, const float* adj_val) {
-  PQI_CHECK_ARG(W && cum && theta_out && n >= 3 && shots > 0);
+  // W is read only without row lists (the dense row scan)
+  PQI_CHECK_ARG((W || adj_ptr) && cum && theta_out && n >= 3 && shots > 0);
   cudaStream_t s = as_stream(stream);
   const int C = (n + 31) / 32;
   const size_t per_warp = (size_t)C * kWtsPitch * sizeof(double);

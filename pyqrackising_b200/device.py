@@ -59,6 +59,38 @@ def stream_ptr(stream=None):
     return ctypes.c_void_p(s.cuda_stream)
 
 
+def pack_bits(bits, n: int, device, stream=None) -> torch.Tensor:
+    """bool[rows, n] (host or device) -> device int32 words, tight pitch
+    ceil(n/32) per row (the reference layout), plus one spare zero word so a
+    single state can also be read as ceil(n/64) 64-bit words."""
+    if isinstance(bits, torch.Tensor):
+        b = bits
+    else:
+        b = torch.from_numpy(np.ascontiguousarray(np.asarray(bits, dtype=np.uint8)))
+    if b.dim() == 1:
+        b = b[None, :]
+    rows = int(b.shape[0])
+    b = b.to(device=device, dtype=torch.uint8).contiguous()
+    n32 = (n + 31) >> 5
+    out = torch.zeros(rows * n32 + 1, dtype=torch.int32, device=device)
+    call("pqi_pack_bits", _ptr(b), rows, n, _ptr(out), stream_ptr(stream))
+    return out
+
+
+def unpack_bits(words: torch.Tensor, n: int, rows: int = 1, pitch: int | None = None, device=None,
+                stream=None) -> np.ndarray:
+    """device words (row pitch `pitch`, default ceil(n/32)) -> host bool[rows, n]."""
+    n32 = (n + 31) >> 5
+    pitch = n32 if pitch is None else pitch
+    w = words[: rows * pitch].view(rows, pitch)
+    if pitch != n32:
+        w = w[:, :n32]
+    w = w.contiguous()
+    out = torch.empty(rows * n, dtype=torch.uint8, device=words.device if device is None else device)
+    call("pqi_unpack_bits", _ptr(w), rows, n, _ptr(out), stream_ptr(stream))
+    return out.view(rows, n).cpu().numpy().astype(np.bool_)
+
+
 class Workspace:
     """Grow-only device scratch buffer handed to the library calls."""
 
@@ -143,28 +175,11 @@ class DeviceGraph:
         """bool[rows, n] (host or device) -> device int32 words, tight pitch
         ceil(n/32) per row (the reference layout), plus one spare zero word so a
         single state can also be read as ceil(n/64) 64-bit words."""
-        if isinstance(bits, torch.Tensor):
-            b = bits
-        else:
-            b = torch.from_numpy(np.ascontiguousarray(np.asarray(bits, dtype=np.uint8)))
-        if b.dim() == 1:
-            b = b[None, :]
-        rows = int(b.shape[0])
-        b = b.to(device=self.device, dtype=torch.uint8).contiguous()
-        out = torch.zeros(rows * self.n32 + 1, dtype=torch.int32, device=self.device)
-        call("pqi_pack_bits", _ptr(b), rows, self.n, _ptr(out), self.sp())
-        return out
+        return pack_bits(bits, self.n, self.device, self.stream)
 
     def unpack(self, words: torch.Tensor, rows: int = 1, pitch: int | None = None) -> np.ndarray:
         """device words (row pitch `pitch`, default ceil(n/32)) -> host bool[rows, n]."""
-        pitch = self.n32 if pitch is None else pitch
-        w = words[: rows * pitch].view(rows, pitch)
-        if pitch != self.n32:
-            w = w[:, : self.n32]
-        w = w.contiguous()
-        out = torch.empty(rows * self.n, dtype=torch.uint8, device=self.device)
-        call("pqi_unpack_bits", _ptr(w), rows, self.n, _ptr(out), self.sp())
-        return out.view(rows, self.n).cpu().numpy().astype(np.bool_)
+        return unpack_bits(words, self.n, rows, pitch, self.device, self.stream)
 
     # -- kernels ---------------------------------------------------------------------
     def gains(self, words: torch.Tensor, rows: int = 1, fp64: bool = True):

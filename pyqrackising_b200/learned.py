@@ -274,31 +274,24 @@ def task_proposals(net: "ProposalNet", dg: D.DeviceGraph, words: torch.Tensor, t
                    mix: float = 0.0):
     """One kick distribution per task, from each task's own state: returns
     (concatenated normalised cumulative arrays, float64; per-task offsets,
-    int64). A proposal p is flattened by the temperature (p^(1/T)) and mixed
-    with the uniform distribution (weight `mix`); a non-finite proposal becomes
-    uniform, so the search never depends on the network being right."""
+    int64). The proposal softmax(logit) flattened by the temperature
+    (softmax(logit / T), i.e. p^(1/T) renormalised) and mixed with the uniform
+    distribution (weight `mix`), built on the device by pqi_mpnn_kick_cdf; a
+    non-finite output becomes uniform, so the search never depends on the
+    network being right."""
     ctx = GraphContext(dg)
     n = dg.n
-    cdfs = []
-    for t in range(words.shape[0]):
-        p = net.proposal(ctx, words[t].contiguous()).to(torch.float64)
-        if not bool(torch.isfinite(p).all().item()) or float(p.sum()) <= 0:
-            p = torch.full((n,), 1.0 / n, dtype=torch.float64, device=p.device)
-        if temperature != 1.0:
-            p = torch.exp(torch.log(p.clamp_min(1e-300)) / temperature)
-            p = p / p.sum()
-        if mix > 0:
-            p = (1.0 - mix) * p + mix / n
-        cdfs.append(proposal_cdf(p))
-    off = torch.arange(len(cdfs), dtype=torch.int64, device=words.device) * n
-    return torch.cat(cdfs).contiguous(), off
-
-
-def proposal_cdf(prob: torch.Tensor) -> torch.Tensor:
-    """Normalised cumulative float64 array of a proposal (the batched search's
-    kick distribution)."""
-    c = torch.cumsum(prob.to(torch.float64), 0)
-    return (c / c[-1]).contiguous()
+    tasks = int(words.shape[0])
+    logits = torch.empty(tasks * n, dtype=torch.float32, device=words.device)
+    for t in range(tasks):
+        F = ctx.features(words[t].contiguous())
+        lg, _ = net.forward(ctx, F)
+        logits[t * n:(t + 1) * n].copy_(lg)
+    cdf = torch.empty(tasks * n, dtype=torch.float64, device=words.device)
+    _lib.call("pqi_mpnn_kick_cdf", _p(logits), n, tasks, ctypes.c_float(temperature), ctypes.c_float(mix), _p(cdf),
+              dg.sp())
+    off = torch.arange(tasks, dtype=torch.int64, device=words.device) * n
+    return cdf, off
 
 
 # ------------------------------------------------------------------------------------

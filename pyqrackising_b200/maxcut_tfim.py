@@ -79,8 +79,9 @@ def _maxcut_tfim(nodes, G_m, quality, shots, is_spin_glass, anneal_t, anneal_h, 
     `jz_matrix` (default G_m) is the matrix whose rows give the sampler's J_eff
     and degrees (the sparse entry point passes the upper triangle, as the
     reference's sparse path reads it); `dg` is G_m already prepared on the
-    device (the solver shares its own)."""
-    n_qubits = len(G_m)
+    device (the solver shares its own; a compressed-row graph, with G_m None,
+    from the sparse entry points)."""
+    n_qubits = dg.n if dg is not None else len(G_m)
 
     if n_qubits < threshold:
         best_solution, best_value = exact_search(G_m, is_spin_glass)
@@ -166,10 +167,14 @@ def hamming_cdf(dg: D.DeviceGraph, quality: int, anneal_t: float, anneal_h: floa
     lib = _lib.load()
     J_eff = torch.empty(n, dtype=torch.float64, device=dev)
     degrees = torch.empty(n, dtype=torch.int32, device=dev)
-    wsp, wsn = dg.wsp(1)
-    # the sparse path passes its stored rows and the reference's float32 rule
-    _lib.call("pqi_tfim_jz_f32" if jz_W is not None else "pqi_tfim_jz",
-              D._ptr(jz_W if jz_W is not None else dg.W), n, D._ptr(J_eff), D._ptr(degrees), wsp, wsn, dg.sp())
+    if hasattr(dg, "tfim_jz"):
+        # a compressed-row graph: its stored rows, the sparse path's float32 rule
+        dg.tfim_jz(J_eff, degrees)
+    else:
+        wsp, wsn = dg.wsp(1)
+        # the sparse path passes its stored rows and the reference's float32 rule
+        _lib.call("pqi_tfim_jz_f32" if jz_W is not None else "pqi_tfim_jz",
+                  D._ptr(jz_W if jz_W is not None else dg.W), n, D._ptr(J_eff), D._ptr(degrees), wsp, wsn, dg.sp())
     thr = torch.from_numpy(init_thresholds(n)).to(dev)
     cum = torch.empty(max(n - 1, 1), dtype=torch.float64, device=dev)
     ws = dg.ws.get(lib.pqi_tfim_cdf_workspace_bytes(n, quality))
@@ -198,6 +203,8 @@ def row_lists(dg: D.DeviceGraph):
     """The nonzero entries of W's rows as device lists (ptr int64[n+1], col
     int32, val float32), built once per prepared graph; None when W is too
     dense for lists to beat the row scan."""
+    if hasattr(dg, "row_lists"):
+        return dg.row_lists()  # a compressed-row graph: its rows are the lists
     if getattr(dg, "_row_lists", False) is not False:
         return dg._row_lists
     n = dg.n
@@ -234,7 +241,7 @@ def sample_batch(dg: D.DeviceGraph, cum, shots: int, repulsion_base: float, seed
     if rl is not None:
         _lib.call(
             "pqi_tfim_sample_adj",
-            D._ptr(dg.W),
+            D._ptr(getattr(dg, "W", None)),
             n,
             D._ptr(rl[0]),
             D._ptr(rl[1]),

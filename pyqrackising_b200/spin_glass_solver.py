@@ -44,16 +44,18 @@ from .util import HEURISTIC_THRESHOLD, as_matrix, get_cut, parse_best_guess
 
 def pair_decode(c: int, n: int):
     """Linear pair index -> (k, l), the reference's enumeration
-    (spin_glass_solver.py:224-234)."""
-    i = 0
-    lcv = n - 1
-    while c >= lcv:
-        c -= lcv
-        i += 1
-        lcv -= 1
-        if not lcv:
-            break
-    return i, c + i + 1
+    (spin_glass_solver.py:224-234): pair (k, l), k < l, has index
+    k(n-1) - k(k-1)/2 + (l-k-1). Closed form, exact for 64-bit indices."""
+    c = int(c)
+    base = lambda k: k * (n - 1) - (k * (k - 1)) // 2  # noqa: E731
+    # largest k with base(k) <= c, from the quadratic, then corrected exactly
+    b = 2 * n - 1
+    k = max(0, min(n - 2, int((b - math.isqrt(max(0, b * b - 8 * c))) // 2)))
+    while k > 0 and base(k) > c:
+        k -= 1
+    while k + 1 <= n - 2 and base(k + 1) <= c:
+        k += 1
+    return k, c - base(k) + k + 1
 
 
 class SearchStats:
@@ -70,11 +72,18 @@ class SearchStats:
         return {"single": self.single, "double": self.double, "gray": self.gray, "rounds": self.rounds}
 
 
-def local_search(dg: D.DeviceGraph, theta, is_spin_glass: bool, gray_iterations: int, gray_seeds: int,
+GRAY_NODE_LIMIT = 131072  # maxcut_tfim_util.py:11: no GPU Gray search above it
+
+
+def local_search(dg, theta, is_spin_glass: bool, gray_iterations: int, gray_seeds: int,
                  mpe: int, max_energy: float, stats: SearchStats | None = None, record_trace: bool = False,
                  max_rounds: int | None = None):
     """Run the reference's GPU-branch loop from bool[n] `theta` on a prepared
-    graph. Returns (device words of the final state, running max_energy)."""
+    graph: a dense ``device.DeviceGraph`` or a CSR ``sparse.SparseDeviceGraph``
+    (the same methods). Above GRAY_NODE_LIMIT nodes the Gray stage is skipped,
+    as the reference's GPU branch has no Gray kernel there
+    (spin_glass_solver_sparse.py:628,752). Returns (device words of the final
+    state, running max_energy)."""
     n = dg.n
     words = dg.pack(theta)
     _, g64 = dg.gains(words)
@@ -113,6 +122,8 @@ def local_search(dg: D.DeviceGraph, theta, is_spin_glass: bool, gray_iterations:
                         stats.trace.append(("double", k, l))
                 continue
         # 3. parallel Gray-code search
+        if n > GRAY_NODE_LIMIT:
+            break
         tout, eout = dg.gray(words, g64, spin, iters_bound, gray_seeds)
         be, bi = dg.select(eout, gray_seeds, 1)
         e = float(be.item())
@@ -177,10 +188,12 @@ def spin_glass_solver(
 
 def _spin_glass_solver(nodes, G_m, quality, shots, best_guess, is_maxcut_gpu, is_spin_glass, anneal_t, anneal_h,
                        repulsion_base, gray_iterations, gray_seed_multiple, bp_scale, bp_damping,
-                       threshold=HEURISTIC_THRESHOLD, jz_matrix=None):
+                       threshold=HEURISTIC_THRESHOLD, jz_matrix=None, graph=None):
     """spin_glass_solver on a dense symmetric matrix; `threshold` and
     `jz_matrix` as in maxcut_tfim._maxcut_tfim (the sparse entry point's
-    values differ)."""
+    values differ). `graph`: an already prepared graph to search on instead
+    of G_m (the sparse entry points' compressed rows, with G_m None; only for
+    graphs above `threshold` and 2 nodes)."""
     n_qubits = len(nodes)
 
     if n_qubits < 3:
@@ -199,7 +212,8 @@ def _spin_glass_solver(nodes, G_m, quality, shots, best_guess, is_maxcut_gpu, is
 
     theta = parse_best_guess(best_guess, n_qubits)
     cut_value = None
-    dg = D.DeviceGraph(G_m)  # prepared once, shared by the seed sampler and the search
+    # prepared once, shared by the seed sampler and the search
+    dg = graph if graph is not None else D.DeviceGraph(G_m)
     if theta is None:
         bitstring, cut_value, _ = _maxcut_tfim(
             list(range(n_qubits)), G_m, quality, shots, is_spin_glass, anneal_t, anneal_h, repulsion_base,

@@ -161,6 +161,11 @@ def evaluate(net: L.ProposalNet | None, n: int = 16384, p: float = 0.01, seed: i
             e, t = plain_from(states[tag])
             res[f"{tag}_then_plain_energy"] = e
             res[f"{tag}_then_plain_s"] = res[f"{tag}_s"] + res["ascent_s"] + t
+    if "learned" in states:
+        # both kick streams from the same optima, each refined, best kept: the
+        # learned starts add to the uniform ones rather than replace them
+        res["both_then_plain_energy"] = max(res["uniform_then_plain_energy"], res["learned_then_plain_energy"])
+        res["both_then_plain_s"] = res["uniform_then_plain_s"] + res["learned_then_plain_s"] - res["ascent_s"]
     return res
 
 

@@ -85,8 +85,7 @@ def test_training_lowers_loss_and_proposals_drive_kicks():
     vA, wA, _, _ = bs.run(tg, w0, 1, rounds=0)
     prob = net.proposal(ctx, wA[0].reshape(-1).contiguous())
     assert torch.isfinite(prob).all() and abs(float(prob.sum()) - 1.0) < 1e-3
-    cdf = L.proposal_cdf(prob)
-    off = torch.zeros(1, dtype=torch.int64, device="cuda")
+    cdf, off = L.task_proposals(net, dg, wA[0:1].contiguous(), temperature=1.0)
     v, _, _, status = bs.run(tg, wA.reshape(-1).contiguous(), 1, rounds=4, kick=8, seed=3, kick_cdf=cdf, cdf_offset=off)
     assert int(status.item()) == 0 and torch.all(v >= vA - 1e-9)
 
@@ -142,3 +141,30 @@ def test_tensor_core_messages_match_cuda_core_messages(n):
     assert np.abs(l1 - l0).max() <= 2e-2 * (np.abs(l0).max() + 1e-6)
     cos = g0 @ g1 / (np.linalg.norm(g0) * np.linalg.norm(g1))
     assert cos > 0.999
+
+
+def test_kick_cdf_kernel():
+    """pqi_mpnn_kick_cdf against float64 numpy: softmax(logit / T) mixed with
+    the uniform distribution, cumulated and normalised; a task with a
+    non-finite logit is uniform."""
+    import ctypes
+
+    from pyqrackising_b200 import _lib
+
+    rng = np.random.default_rng(3)
+    n, tasks, T, mix = 3001, 3, 2.5, 0.1
+    z = rng.standard_normal((tasks, n)).astype(np.float32) * 4
+    z[2, 17] = np.nan
+    cdf = torch.empty(tasks * n, dtype=torch.float64, device="cuda")
+    _lib.call("pqi_mpnn_kick_cdf", ctypes.c_void_p(torch.from_numpy(z).cuda().data_ptr()), n, tasks,
+              ctypes.c_float(T), ctypes.c_float(mix), ctypes.c_void_p(cdf.data_ptr()), None)
+    got = cdf.cpu().numpy().reshape(tasks, n)
+    for t in range(tasks):
+        if t == 2:
+            p = np.full(n, 1.0 / n)
+        else:
+            e = np.exp(z[t].astype(np.float64) / T - (z[t].astype(np.float64) / T).max())
+            p = (1 - mix) * e / e.sum() + mix / n
+        c = np.cumsum(p)
+        np.testing.assert_allclose(got[t], c / c[-1], rtol=1e-12, atol=1e-12)
+        assert got[t][-1] == 1.0
