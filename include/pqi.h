@@ -422,6 +422,13 @@ pqi_status pqi_mpnn_norm_adj(const float* W, int n, void* Ahat, int ld, float* s
 pqi_status pqi_mpnn_features(const uint32_t* theta, const double* gains64, const float* s,
                              float mean_s, int n, void* F, void* stream);
 
+/* Gradient clipping: *norm_out (nullable) = the L2 norm of g (float64
+ * accumulation); when it exceeds max_norm > 0, g is scaled to max_norm. */
+pqi_status pqi_mpnn_grad_clip(float* g, size_t count, float max_norm, float* norm_out, void* stream);
+
+/* *out = sum of count floats, float64, fixed order (one block). */
+pqi_status pqi_mpnn_sum(const float* x, size_t count, double* out, void* stream);
+
 /* Kick distributions of `tasks` states from their logits (tasks x n,
  * contiguous): softmax(logit / temperature) in float64, mixed with the
  * uniform distribution ((1 - mix) p + mix / n), as normalised cumulative

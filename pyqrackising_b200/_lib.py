@@ -121,6 +121,8 @@ SIGNATURES = {
     "pqi_mpnn_features": (_i, [_vp, _vp, _vp, ctypes.c_float, _i, _vp, _vp]),
     "pqi_mpnn_softmax_xent": (_i, [_vp, _vp, _i, _vp, _vp, _vp, _vp]),
     "pqi_mpnn_kick_cdf": (_i, [_vp, _i, _i, ctypes.c_float, ctypes.c_float, _vp, _vp]),
+    "pqi_mpnn_grad_clip": (_i, [_vp, _sz, ctypes.c_float, _vp, _vp]),
+    "pqi_mpnn_sum": (_i, [_vp, _sz, _vp, _vp]),
     "pqi_mpnn_relu_bwd": (_i, [_vp, _vp, _sz, _vp, _vp, _vp]),
     "pqi_mpnn_colsum": (_i, [_vp, _i, _i, _i, _vp, _i, _vp]),
     "pqi_mpnn_to_bf16": (_i, [_vp, _sz, _vp, _vp]),

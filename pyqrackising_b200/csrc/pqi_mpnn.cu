@@ -323,7 +323,62 @@ __global__ void __launch_bounds__(1024) kick_cdf_kernel(const float* __restrict_
   for (int v = threadIdx.x; v < n; v += blockDim.x) out[v] = out[v] / last;
 }
 
+// One block: sum of squares (float64) of count floats, then, when its root
+// exceeds max_norm > 0, every element scaled by max_norm / norm.
+__global__ void __launch_bounds__(1024) grad_clip_kernel(float* __restrict__ g, size_t count,
+                                                         float max_norm, float* __restrict__ norm_out) {
+  __shared__ double red[32];
+  __shared__ double s_norm;
+  double acc = 0.0;
+  for (size_t i = threadIdx.x; i < count; i += blockDim.x) acc += (double)g[i] * (double)g[i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    s_norm = sqrt(t);
+    if (norm_out) *norm_out = (float)s_norm;
+  }
+  __syncthreads();
+  const double norm = s_norm;
+  if (max_norm > 0.0f && norm > (double)max_norm) {
+    const float scale = (float)((double)max_norm / norm);
+    for (size_t i = threadIdx.x; i < count; i += blockDim.x) g[i] *= scale;
+  }
+}
+
+// Sum of count floats in float64 (one block, fixed order).
+__global__ void __launch_bounds__(1024) sum_kernel(const float* __restrict__ x, size_t count,
+                                                   double* __restrict__ out) {
+  __shared__ double red[32];
+  double acc = 0.0;
+  for (size_t i = threadIdx.x; i < count; i += blockDim.x) acc += (double)x[i];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+    *out = t;
+  }
+}
+
 extern "C" {
+
+pqi_status pqi_mpnn_grad_clip(float* g, size_t count, float max_norm, float* norm_out, void* stream) {
+  PQI_CHECK_ARG(g && count > 0 && max_norm >= 0.0f);
+  grad_clip_kernel<<<1, 1024, 0, as_stream(stream)>>>(g, count, max_norm, norm_out);
+  PQI_LAUNCHED("grad_clip_kernel");
+  return PQI_OK;
+}
+
+pqi_status pqi_mpnn_sum(const float* x, size_t count, double* out, void* stream) {
+  PQI_CHECK_ARG(x && out && count > 0);
+  sum_kernel<<<1, 1024, 0, as_stream(stream)>>>(x, count, out);
+  PQI_LAUNCHED("sum_kernel");
+  return PQI_OK;
+}
 
 pqi_status pqi_mpnn_kick_cdf(const float* logits, int n, int tasks, float temperature, float mix,
                              double* cdf, void* stream) {

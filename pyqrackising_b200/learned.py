@@ -65,7 +65,9 @@ class GraphContext:
         self.Ah = torch.empty(n * self.ld, dtype=torch.bfloat16, device=dg.device)
         self.s = torch.empty(n, dtype=torch.float32, device=dg.device)
         _lib.call("pqi_mpnn_norm_adj", _p(dg.W), n, _p(self.Ah), self.ld, _p(self.s), dg.sp())
-        self.mean_s = float(self.s.mean().item())
+        total = torch.empty(1, dtype=torch.float64, device=dg.device)
+        _lib.call("pqi_mpnn_sum", _p(self.s), n, _p(total), dg.sp())
+        self.mean_s = float(total.item()) / n
 
     def features(self, words: torch.Tensor, g64: torch.Tensor | None = None) -> torch.Tensor:
         if g64 is None:
@@ -210,10 +212,10 @@ class ProposalNet:
 
     def clip_grad(self, max_norm: float) -> float:
         """Scale the gradient to at most `max_norm` (L2); returns the norm before."""
-        norm = float(torch.linalg.vector_norm(self.g).item())
-        if norm > max_norm > 0:
-            self.g.mul_(max_norm / norm)
-        return norm
+        norm = torch.empty(1, dtype=torch.float32, device=self.device)
+        _lib.call("pqi_mpnn_grad_clip", _p(self.g), self.count, ctypes.c_float(max(0.0, float(max_norm))), _p(norm),
+                  None)
+        return float(norm.item())
 
     def adam_step(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8, stream=None):
         self.step_count += 1
