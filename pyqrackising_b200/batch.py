@@ -28,7 +28,12 @@ class BatchedSearch:
 
     def __init__(self, graphs: list[D.DeviceGraph], stream=None, row_lists: bool = True):
         """row_lists: give sparse graphs (at most a quarter of W nonzero) their
-        row lists, so the CTA form's starting fields cost O(nonzeros)."""
+        row lists, so the CTA form's starting fields cost O(nonzeros). A float
+        graph below 2048 nodes then sums its starting fields in column order
+        instead of by warp shuffles: the same values up to float64 rounding, so
+        its search may end at a different (still local, float64-exact) optimum
+        than with row_lists=False; integer graphs and float graphs of 2048+
+        nodes give identical searches either way."""
         if not graphs:
             raise ValueError("no graphs")
         kinds = {g.w.kind for g in graphs}

@@ -313,6 +313,13 @@ def test_row_list_starts_match_dense_starts():
         dgs = [DeviceGraph(W) for W in Ws]
         with_lists = BatchedSearch(dgs)
         dense = BatchedSearch(dgs, row_lists=False)
+        # the lists are really attached (these graphs are at most 10 % nonzero),
+        # and really absent from the dense descriptors
+        from pyqrackising_b200.batch import _DESC
+
+        adj = np.frombuffer(with_lists.desc.cpu().numpy().tobytes(), dtype=_DESC)["adj_ptr"]
+        assert np.all(adj != 0)
+        assert np.all(np.frombuffer(dense.desc.cpu().numpy().tobytes(), dtype=_DESC)["adj_ptr"] == 0)
         task_graph = [i % len(Ws) for i in range(3 * len(Ws))]
         words = with_lists.random_states(task_graph, seed=9)
         for variant in ("cta", "cta64"):
