@@ -421,6 +421,51 @@ def time_to_best_learned(n=8192, starts=32, cluster=8, rounds=4, kick=64, temper
     }
 
 
+def scoring_batch_leg(dg, batch=4096, reps=50):
+    """The scoring kernel at config 2's own parallel seed count (4096
+    candidates, a GEMM 16x smaller than the headline's): device time per call
+    (CUDA events around the GEMM launch and around the whole call), the
+    fraction of the int8 peak, L2 flushed before each call."""
+    import torch
+
+    from oracle import oracle as O
+    from pyqrackising_b200 import _lib
+
+    X = np.random.default_rng(77).random((batch, N_NODES)) < 0.5
+    words = dg.pack(X)
+    G, L = O.cut_geometry(batch, 148)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dg.device)
+    for _ in range(5):
+        dg.calculate_cut(words, batch, False, G, L, energies=False)
+    k_ms, s_ms = [], []
+    lib = _lib.load()
+    for i in range(reps):
+        flush.fill_(i & 0xFF)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ka, kb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        ka.record()
+        kb.record()
+        lib.pqi_score_set_events(ctypes.c_void_p(ka.cuda_event), ctypes.c_void_p(kb.cuda_event))
+        dg.calculate_cut(words, batch, False, G, L, energies=False)
+        b.record()
+        b.synchronize()
+        k_ms.append(ka.elapsed_time(kb))
+        s_ms.append(a.elapsed_time(b))
+    lib.pqi_score_set_events(None, None)
+    _, bf16, src = peaks()
+    km = float(np.median(k_ms))
+    ops = 2.0 * batch * N_NODES * N_NODES
+    return {
+        "workload": f"ER G(n=2048,p=0.5) unit weights, {batch} candidates per call (config 2's parallel seeds)",
+        "kernel_ms": km,
+        "call_ms": float(np.median(s_ms)),
+        "candidates_per_s": batch / (float(np.median(s_ms)) / 1e3),
+        "frac_of_int8_peak": ops / (km / 1e3) / 1e12 / (2.0 * bf16),
+        "peak_basis": f"int8 dense = 2 x bf16 dense ({src} bf16 {bf16} TFLOP/s)",
+    }
+
+
 def e2e_pipeline(dg, batches_host, like, G, L, steps, warmup):
     """Device time (ms) of `steps` end-to-end steps: H2D copy of the step's
     packed batch from pinned memory, scoring through the public call, D2H of
@@ -1054,6 +1099,8 @@ def main():
     }
     if rank == 0:
         line["clocks"] = clocks.summary()
+        if world == 1:
+            line["scoring_b4096"] = scoring_batch_leg(dg)
         if world == 1 and not args.no_ttb:
             line["time_to_best"] = time_to_best()
             line["time_to_best_learned"] = time_to_best_learned()
