@@ -900,7 +900,8 @@ def leg_cluster(n=8192, starts=8):
     tasks = [0] * starts
     w0 = bs.random_states(tasks, seed=7)
     v, best, flips, st = bs.cluster_ascent(tasks, w0, True, cluster_size=8)
-    v2, best2, flips2, st2 = bs.run(tasks, w0, True, rounds=0)
+    # the cluster form keeps float64 fields: compare with the CTA form's float64 fields
+    v2, best2, flips2, st2 = bs.run(tasks, w0, True, rounds=0, fields="f64")
     torch.cuda.synchronize()
     ok = torch.equal(best, best2) and int(st.item()) == 0
     _emit(leg="cluster", flips=int(flips.item()), best=float(v.max()), matches_batched=ok)
