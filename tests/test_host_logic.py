@@ -28,6 +28,17 @@ def test_pair_decode_matches_reference_loop(oracle_mod):
                 c += 1
 
 
+def test_pair_decode_64_bit_indices():
+    """The closed form at sizes whose pair count exceeds int32 (the
+    compressed-row double pass reports 64-bit pair indices)."""
+    rng = np.random.default_rng(0)
+    for n in (46341, 46342, 200000, 1 << 20):
+        total = n * (n - 1) // 2
+        for c in [0, 1, total - 1, total // 2] + [int(x) for x in rng.integers(0, total, 50)]:
+            k, l = S.pair_decode(c, n)
+            assert 0 <= k < l < n and k * (n - 1) - k * (k - 1) // 2 + (l - k - 1) == c
+
+
 def test_best_guess_parsing():
     n = 8
     assert util.parse_best_guess("10110000", n).tolist() == [True, False, True, True, False, False, False, False]
