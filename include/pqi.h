@@ -64,6 +64,9 @@ typedef struct {
   int ld;
   int kind;              /* pqi_wkind */
   double upper_sum;      /* sum_{u<v} W_uv (host value, filled by pqi_prepare_weights) */
+  const int8_t* W_d;     /* PQI_W_F32 (optional, pqi_prepare_digits): 3*n*ld int8, the
+                            fixed-point digit planes of W_f32z, else NULL */
+  double wscale;         /* W_f32z ~= wscale * (d0 2^16 + d1 2^8 + d2) (pqi_prepare_digits) */
 } pqi_weights;
 
 /* ---------------------------------------------------------------------------
@@ -117,11 +120,28 @@ pqi_status pqi_prepare_weights(const float* W, int n, const pqi_weight_stats* st
                                float* W_f32z, int8_t* W_i8, uint16_t* W_hi, uint16_t* W_lo,
                                pqi_weights* out_host, void* stream);
 
+/*
+ * Fixed-point digit planes of float weights, for exact tensor-core scoring:
+ * W_f32z times 2^S (S the largest integer with maxabs * 2^S < 2^22 - 1) is
+ * rounded to integers v, |v| < 2^22, and split into balanced int8 digits,
+ * v = d0 2^16 + d1 2^8 + d2 (d in [-128, 127]); planes d0, d1, d2 of n*ld bytes
+ * each go to W_d (3*n*ld bytes). Fills w->W_d and w->wscale = 2^-S. The
+ * scoring GEMM then accumulates each plane exactly in int32 and combines them
+ * in 64-bit integers, so the only error of a score is the rounding of W to
+ * multiples of 2^-S (at most 2^-S / 2 per weight). maxabs = max |W_ij| off the
+ * diagonal (pqi_weight_stats.maxabs). No reference counterpart (the
+ * reference sums float32 weights in float32).
+ */
+pqi_status pqi_prepare_digits(pqi_weights* w, float maxabs, int8_t* W_d, void* stream);
+
 /* Select the batched-scoring implementation: 0 = tensor cores (tcgen05, the
  * default; the kernel expands the packed candidates into its +-1 operand
- * tiles itself), 1 = CUDA cores, 2 = tensor cores fed by a separate expansion
- * pass, 3 = as 2 with CTA pairs (cta_group::2 MMAs) for batches of more than
- * 128 candidates. Process-wide; used to cross-check the implementations. */
+ * tiles itself; float weights as their int8 digit planes when prepared, with
+ * exact integer accumulation), 1 = CUDA cores, 2 = tensor cores fed by a
+ * separate expansion pass, 3 = as 2 with CTA pairs (cta_group::2 MMAs) for
+ * batches of more than 128 candidates, 4 = as 0 but float weights as split
+ * bf16 (hi + lo) with float32 accumulation. Process-wide; used to
+ * cross-check the implementations. */
 pqi_status pqi_score_set_path(int path);
 
 /* Record two caller-owned cudaEvent_t on the call's stream immediately before

@@ -49,6 +49,8 @@ class PqiWeights(ctypes.Structure):
         ("ld", ctypes.c_int),
         ("kind", ctypes.c_int),
         ("upper_sum", ctypes.c_double),
+        ("W_d", ctypes.c_void_p),
+        ("wscale", ctypes.c_double),
     ]
 
 
@@ -95,6 +97,7 @@ SIGNATURES = {
     "pqi_padded_ld": (_i, [_i]),
     "pqi_scan_weights": (_i, [_vp, _i, _vp, _sz, ctypes.POINTER(PqiWeightStats), _vp]),
     "pqi_prepare_weights": (_i, [_vp, _i, ctypes.POINTER(PqiWeightStats), _vp, _vp, _vp, _vp, _WP, _vp]),
+    "pqi_prepare_digits": (_i, [_WP, ctypes.c_float, _vp, _vp]),
     "pqi_score_set_path": (_i, [_i]),
     "pqi_score_set_events": (_i, [_vp, _vp]),
     "pqi_score_set_grid": (_i, [_i]),

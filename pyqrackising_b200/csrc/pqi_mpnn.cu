@@ -243,7 +243,7 @@ using namespace pqi;
 // logit makes the task's distribution uniform (the search must not depend on
 // the network being right).
 __global__ void __launch_bounds__(1024) kick_cdf_kernel(const float* __restrict__ logits, int n,
-                                                        float inv_t, float mix,
+                                                        double temp, float mix,
                                                         double* __restrict__ cdf) {
   __shared__ double sred[32];
   __shared__ double s_bcast;
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(1024) kick_cdf_kernel(const float* __restrict_
   for (int v = threadIdx.x; v < n; v += blockDim.x) {
     const float x = z[v];
     if (!isfinite(x)) s_bad = 1;
-    m = fmax(m, (double)x * (double)inv_t);
+    m = fmax(m, (double)x / temp);
   }
   for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
   if (lane == 0) sred[warp] = m;
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(1024) kick_cdf_kernel(const float* __restrict_
   // 2. sum of the unnormalised weights
   double sum = 0.0;
   for (int v = threadIdx.x; v < n; v += blockDim.x)
-    sum += uniform ? 1.0 : exp((double)z[v] * (double)inv_t - zmax);
+    sum += uniform ? 1.0 : exp((double)z[v] / temp - zmax);
   for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
   if (lane == 0) sred[warp] = sum;
   __syncthreads();
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(1024) kick_cdf_kernel(const float* __restrict_
     const int v = base + threadIdx.x;
     double p = 0.0;
     if (v < n) {
-      const double w = uniform ? 1.0 : exp((double)z[v] * (double)inv_t - zmax);
+      const double w = uniform ? 1.0 : exp((double)z[v] / temp - zmax);
       p = (1.0 - (double)mix) * (w / total) + (double)mix / (double)n;
     }
     double x = p;
@@ -383,7 +383,7 @@ pqi_status pqi_mpnn_sum(const float* x, size_t count, double* out, void* stream)
 pqi_status pqi_mpnn_kick_cdf(const float* logits, int n, int tasks, float temperature, float mix,
                              double* cdf, void* stream) {
   PQI_CHECK_ARG(logits && cdf && n > 0 && tasks > 0 && temperature > 0.0f && mix >= 0.0f && mix <= 1.0f);
-  kick_cdf_kernel<<<tasks, 1024, 0, as_stream(stream)>>>(logits, n, 1.0f / temperature, mix, cdf);
+  kick_cdf_kernel<<<tasks, 1024, 0, as_stream(stream)>>>(logits, n, (double)temperature, mix, cdf);
   PQI_LAUNCHED("kick_cdf_kernel");
   return PQI_OK;
 }

@@ -122,7 +122,9 @@ template <bool kInt8, bool PAIR, bool FUSED>
 __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
     score_tc_kernel(const __grid_constant__ CUtensorMap map_a,
                     const __grid_constant__ CUtensorMap map_b0,
-                    const __grid_constant__ CUtensorMap map_b1, int n, int shots,
+                    const __grid_constant__ CUtensorMap map_b1,
+                    const __grid_constant__ CUtensorMap map_b2, int planes, double qscale,
+                    int n, int shots,
                     const uint32_t* __restrict__ theta, int n32, double upper_sum, int spin,
                     SelGeom geo, double* __restrict__ qpart, float* __restrict__ energies,
                     unsigned int* __restrict__ mcount, unsigned int* __restrict__ mdone,
@@ -158,7 +160,12 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
   const int t_begin = (int)(((long long)unit * ntiles) / units);
   const int t_end = (int)(((long long)(unit + 1) * ntiles) / units);
   const int kb_per_pass = kInt8 ? (n + BK_BYTES - 1) / BK_BYTES : (n + 63) / 64;
-  const int kblocks = kInt8 ? kb_per_pass : 2 * kb_per_pass;
+  // int8 operands: `planes` K passes, each its own accumulation (planes = 3:
+  // the digit planes of float weights, combined exactly in the epilogue);
+  // bf16: the hi and lo passes accumulate into one accumulator
+  const int upt = kInt8 ? planes : 1;                       // accumulations per tile
+  const int spu = kInt8 ? kb_per_pass : 2 * kb_per_pass;    // stages per accumulation
+  const int kblocks = upt * spu;                            // stages per tile
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NST; ++s) {
@@ -203,6 +210,7 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
       bool ok = true;
       for (int t = t_begin; t < t_end && ok; ++t) {
         const int m0 = (t / ntn) * UM + rank * BM, n0 = (t % ntn) * BN + rank * (BN / 2);
+        int kp = 0, pass = 0;  // K block within its pass, pass (plane, or hi / lo)
         for (int kb = 0; kb < kblocks; ++kb, ++it) {
           const int s = it % NST;
           if (it >= NST && !mbar_wait(&empty_bar[s], ((it / NST) - 1) & 1)) {
@@ -210,8 +218,12 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
             s_fail = 1;
             break;
           }
-          const int kk = kInt8 ? kb * BK_BYTES : (kb % kb_per_pass) * 64;
-          const CUtensorMap* mb = (kInt8 || kb < kb_per_pass) ? &map_b0 : &map_b1;
+          const int kk = kInt8 ? kp * BK_BYTES : kp * 64;
+          const CUtensorMap* mb = pass == 0 ? &map_b0 : (pass == 1 ? &map_b1 : &map_b2);
+          if (++kp == kb_per_pass) {
+            kp = 0;
+            ++pass;
+          }
           uint8_t* dst = smem + s * SB;
           if constexpr (PAIR) {
             // both CTAs' bytes count on the even CTA's barrier, armed there
@@ -238,7 +250,8 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
       uint32_t it = 0;
       int i = 0;
       bool ok = true;
-      for (int t = t_begin; t < t_end && ok; ++t, ++i) {
+      const int units_total = (t_end - t_begin) * upt;
+      for (int u = 0; u < units_total && ok; ++u, ++i) {
         const int a = i & 1;
         if (i >= 2 && !mbar_wait(&acce_bar[a], ((i >> 1) - 1) & 1)) {
           ok = false;
@@ -246,7 +259,7 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tmem_d = tmem_base + (uint32_t)(a * BN);
-        for (int kb = 0; kb < kblocks; ++kb, ++it) {
+        for (int kb = 0; kb < spu; ++kb, ++it) {
           const int s = it % NST;
           if (!mbar_wait(&full_bar[s], (it / NST) & 1)) {
             ok = false;
@@ -285,40 +298,52 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
     __syncwarp();
   } else if (FUSED && warp >= 6) {
     // ---- A producers: warps 6-9, thread p writes row p of every A tile ----
-    // Stage it of this CTA is tile t_begin + it / kblocks, K block
-    // it % kblocks. The row's packed words for stage it + PF are copied into
+    // Stages run tile by tile, kblocks per tile, K blocks within each pass in
+    // order. The row's packed words for stage it + PF are copied into
     // the thread's ring slot while stage it is expanded, so the L2 latency of
     // the bits is hidden behind PF stages of MMAs.
     const int p = threadIdx.x - 192;
     constexpr int WPS = kInt8 ? 4 : 2;  // packed words per stage
-    const long long nstage = (long long)(t_end - t_begin) * kblocks;
+    const int nstage = (t_end - t_begin) * kblocks;
     const uint32_t ring = smem_u32(smem + NST * SB) + (uint32_t)p * 16u;
-    auto issue = [&](long long st) {
-      if (st < nstage) {
-        const int t = t_begin + (int)(st / kblocks), kb = (int)(st % kblocks);
-        const int b = (t / ntn) * BM + p;
-        const int w0 = kInt8 ? kb * 4 : (kb % kb_per_pass) * 2;
+    // the stage being prefetched: tile ti, K block ki, ring slot si (all
+    // advanced by one per issue, no divisions in the loop)
+    int ti = t_begin, ki = 0, kp = 0, si = 0, issued = 0;
+    auto issue = [&]() {
+      if (issued < nstage) {
+        const int b = (ti / ntn) * BM + p;
+        const int w0 = kp * (kInt8 ? 4 : 2);  // the stage's first word within the row
         const uint32_t* src = theta + (size_t)(b < shots ? b : 0) * n32;
-        const uint32_t dst = ring + (uint32_t)((st % PF) * 128 * 16);
+        const uint32_t dst = ring + (uint32_t)si * (128u * 16u);
 #pragma unroll
         for (int q = 0; q < WPS; ++q)
           cp_async4(dst + 4 * q, src + min(w0 + q, n32 - 1), b < shots && w0 + q < n32);
+        if (++kp == kb_per_pass) kp = 0;
+        if (++ki == kblocks) {
+          ki = 0;
+          kp = 0;
+          ++ti;
+        }
+        ++issued;
       }
       cp_async_commit();  // an empty group past the end keeps the count uniform
+      if (++si == PF) si = 0;
     };
 #pragma unroll 1
-    for (int q = 0; q < PF; ++q) issue(q);
+    for (int q = 0; q < PF; ++q) issue();
     bool ok = true;
+    int slot_i = 0, s = 0;
+    uint32_t phase = 0;  // parity of the ring pass of stage s
 #pragma unroll 1
-    for (long long st = 0; st < nstage; ++st) {
+    for (int st = 0; st < nstage; ++st) {
       cp_async_wait<PF - 1>();  // this stage's words have landed
       uint32_t wd[4];
-      const uint8_t* slot = smem + NST * SB + (size_t)p * 16 + (size_t)(st % PF) * 128 * 16;
+      const uint8_t* slot = smem + NST * SB + (size_t)p * 16 + (size_t)slot_i * (128 * 16);
 #pragma unroll
       for (int q = 0; q < 4; ++q) wd[q] = (q < WPS) ? *reinterpret_cast<const volatile uint32_t*>(slot + 4 * q) : 0u;
-      issue(st + PF);
-      const int s = (int)(st % NST);
-      if (st >= NST && !mbar_wait(&empty_bar[s], (uint32_t)((st / NST) - 1) & 1u)) {
+      if (++slot_i == PF) slot_i = 0;
+      issue();
+      if (st >= NST && !mbar_wait(&empty_bar[s], phase ^ 1u)) {
         ok = false;
         s_fail = 1;
       }
@@ -346,6 +371,10 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
       __syncwarp();
       if (!__all_sync(0xFFFFFFFFu, ok)) break;
       if (lane == 0) mbar_arrive(&full_bar[s]);
+      if (++s == NST) {
+        s = 0;
+        phase ^= 1u;
+      }
     }
     cp_async_wait<0>();
   } else {
@@ -356,8 +385,7 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
     long long qacc_i = 0;
     double qacc_f = 0.0;
     int i = 0;
-    for (int t = t_begin; t < t_end; ++t, ++i) {
-      const int a = i & 1;
+    for (int t = t_begin; t < t_end; ++t) {
       const int tm = t / ntn, tn = t % ntn;                // tile row, node tile
       const int tm128 = tm * (PAIR ? 2 : 1) + rank;          // this CTA's 128-candidate block
       const int b = tm128 * BM + row, n0 = tn * BN;
@@ -375,11 +403,15 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
           xbits[c] = (b < shots && j0 < n) ? __ldg(th + (j0 >> 5)) : 0u;
         }
       }
+      // the tile's q over its accumulations (digit planes: sum_p q_p 2^(8(P-1-p)),
+      // exact in 64 bits)
+      long long qt_i = 0;
+      double qt_f = 0.0;
+      for (int pl = 0; pl < upt; ++pl, ++i) {
+      const int a = i & 1;
       // columns beyond n hold zeros (TMA zero fill of W), so no column mask
       const bool ready = mbar_wait(&accf_bar[a], (i >> 1) & 1);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      long long qt_i = 0;
-      double qt_f = 0.0;
       if (__all_sync(0xFFFFFFFFu, ready)) {
         const uint32_t tbase =
             tmem_base + (uint32_t)(a * BN) + ((uint32_t)(quarter * 32) << 16);
@@ -445,9 +477,9 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
         }
         // int8: sum_j x_bj Y_bj = 2 * (sum over x = +1) - (sum over all)
         if constexpr (kInt8) {
-          qt_i = 2ll * (long long)s_set - (long long)s_all;
+          qt_i += (2ll * (long long)s_set - (long long)s_all) << (8 * (upt - 1 - pl));
         } else {
-          qt_f = f_q;
+          qt_f += f_q;
         }
       } else {
         s_fail = 1;
@@ -461,6 +493,7 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
           mbar_arrive(&acce_bar[a]);
         }
       }
+      }  // accumulations of the tile
       bool finish = false;  // this CTA folds block tm into the selection
       double q = 0.0;
       if (whole) {
@@ -468,7 +501,7 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
         qacc_f += qt_f;
         if (t == last) {
           finish = tm128 < ntm;  // (a pair's odd half can lie wholly past the batch)
-          q = kInt8 ? (double)qacc_i : qacc_f;
+          q = kInt8 ? (double)qacc_i * qscale : qacc_f;
           qacc_i = 0;
           qacc_f = 0.0;
         }
@@ -488,6 +521,7 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
             finish = true;
             if (b < shots) {
               for (int u = 0; u < ntn; ++u) q += __ldcg(qpart + (size_t)u * shots + b);
+              if constexpr (kInt8) q *= qscale;
             }
           }
           epi_barrier();  // s_bcast is rewritten by a later block
@@ -670,7 +704,13 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
   }
   if (!arch_ok || !encode_fn()) return PQI_ENOTSUP;
   const int n = w->n, n32 = (n + 31) >> 5, ld = w->ld;
-  const bool i8 = w->kind == PQI_W_I8;
+  // int8 tensor-core operands: integer weights (one plane), or float weights
+  // as three fixed-point digit planes (exact integer sums, scaled by wscale);
+  // path 4 scores float weights as split bf16 instead
+  const bool digits = w->kind != PQI_W_I8 && w->W_d && g_score_path != 4;
+  const bool i8 = w->kind == PQI_W_I8 || digits;
+  const int planes = digits ? 3 : 1;
+  const double qscale = digits ? w->wscale : 1.0;
   // the int8 epilogue sums 256 columns of |Y| <= 127 n in 32 bits
   if (i8 && n > 65536) return PQI_ENOTSUP;
   const int ntn = (n + tc::BN - 1) / tc::BN;
@@ -678,7 +718,7 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
   // 0 (default): single CTAs that expand the packed candidates into the A
   // tiles themselves; 2: single CTAs, A expanded by a separate pass and loaded
   // by TMA; 3: CTA pairs (cta_group::2), A as in 2
-  const bool fused = g_score_path == 0;
+  const bool fused = g_score_path == 0 || g_score_path == 4;
   const bool pair = g_score_path == 3 && ntm >= 2;
   // one zeroed control block: err, mdone, key, then mcount[ntm]
   const size_t ctl_bytes = 64 + (size_t)ntm * sizeof(unsigned);
@@ -693,16 +733,21 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
   unsigned long long* key = reinterpret_cast<unsigned long long*>(ctl + 16);
   unsigned* mcount = reinterpret_cast<unsigned*>(ctl + 64);
   if (i8) {
-    if (!w->W_i8) return PQI_EINVAL;
+    if (!digits && !w->W_i8) return PQI_EINVAL;
   } else if (!w->W_hi || !w->W_lo) {
     return PQI_EINVAL;
   }
   const int brows = pair ? tc::BN / 2 : tc::BN;
-  CUtensorMap ma, mb0, mb1;
-  if (!cached_map(&mb0, i8 ? (const void*)w->W_i8 : (const void*)w->W_hi, i8, n, n, ld, brows))
-    return PQI_ENOTSUP;
-  if (!cached_map(&mb1, i8 ? (const void*)w->W_i8 : (const void*)w->W_lo, i8, n, n, ld, brows))
-    return PQI_ENOTSUP;
+  // the B operand's maps: int8 weights (all three the same), digit planes
+  // 0..2 (n*ld bytes apart), or bf16 hi and lo
+  const size_t plane_bytes = (size_t)n * ld;
+  const void* b0 = digits ? (const void*)w->W_d : (i8 ? (const void*)w->W_i8 : (const void*)w->W_hi);
+  const void* b1 = digits ? (const void*)(w->W_d + plane_bytes) : (i8 ? b0 : (const void*)w->W_lo);
+  const void* b2 = digits ? (const void*)(w->W_d + 2 * plane_bytes) : b1;
+  CUtensorMap ma, mb0, mb1, mb2;
+  if (!cached_map(&mb0, b0, i8, n, n, ld, brows)) return PQI_ENOTSUP;
+  if (!cached_map(&mb1, b1, i8, n, n, ld, brows)) return PQI_ENOTSUP;
+  if (!cached_map(&mb2, b2, i8, n, n, ld, brows)) return PQI_ENOTSUP;
   if (fused) {
     ma = mb0;  // not read: the kernel writes its A tiles itself
   } else if (!cached_map(&ma, X, i8, shots, n, ld, tc::BM)) {
@@ -759,11 +804,11 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     const int pairs = std::max(1, std::min({tiles, limit / 2, fit[i8]}));
     cfg.gridDim = dim3(2 * pairs);
     if (i8) {
-      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<true, true, false>, ma, mb0, mb1, n, shots,
+      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<true, true, false>, ma, mb0, mb1, mb2, planes, qscale, n, shots,
                                  theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
                                  mdone, key, best_energy, best_index, err));
     } else {
-      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<false, true, false>, ma, mb0, mb1, n, shots,
+      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<false, true, false>, ma, mb0, mb1, mb2, planes, qscale, n, shots,
                                  theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
                                  mdone, key, best_energy, best_index, err));
     }
@@ -772,12 +817,12 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     const int threads = fused ? tc::FTHREADS : tc::PTHREADS;
     if (i8) {
       auto k = fused ? tc::score_tc_kernel<true, false, true> : tc::score_tc_kernel<true, false, false>;
-      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo,
+      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, mb2, planes, qscale, n, shots, theta, n32, w->upper_sum, spin, geo,
                                           qpart, energies, mcount, mdone, key, best_energy, best_index,
                                           err);
     } else {
       auto k = fused ? tc::score_tc_kernel<false, false, true> : tc::score_tc_kernel<false, false, false>;
-      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, n, shots, theta, n32, w->upper_sum, spin, geo,
+      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, mb2, planes, qscale, n, shots, theta, n32, w->upper_sum, spin, geo,
                                           qpart, energies, mcount, mdone, key, best_energy, best_index,
                                           err);
     }

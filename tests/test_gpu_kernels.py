@@ -153,8 +153,15 @@ def test_gray(name, oracle_mod):
         else:
             tol = 1e-5 * np.abs(W.astype(np.float64)).sum() / 2
             assert np.all(np.abs(e - d[f"kcl_gray_{S}_energy"]) <= tol)
+            # a seed may end elsewhere than the reference's only if its walk
+            # made a keep-or-revert decision on a gain within float32 rounding
+            # of zero (the oracle reproduces the reference's walk and reports
+            # each seed's smallest |gain|)
             same = np.all(t == d[f"kcl_gray_{S}_theta"], axis=1)
-            assert same.mean() >= 0.99
+            rt, _, _, margin = oracle_mod.gray(W, oracle_mod.pack64(th), spin, T, S, margins=True)
+            assert np.array_equal(rt, d[f"kcl_gray_{S}_theta"])
+            row_scale = float(np.abs(W.astype(np.float64)).sum(axis=1).mean())
+            assert np.all(same | (margin <= 1e-5 * row_scale))
 
 
 def test_descent_matches_repeated_single_passes(oracle_mod):
