@@ -378,6 +378,11 @@ __global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
     for (int i = 0; i < DR; ++i) {
       // c = -2 when bits k and l agree: cl already is for x_k = +1; x_k = -1 flips its sign
       const uint32_t flip = (((xk >> i) & 1u) ^ 1u) << 31;
+      // (t, j) = (c mod G, c / G) of the first pair of the row that reaches the
+      // exact path (column e0), then advanced along the row's columns
+      bool have_tj = false;
+      uint32_t t0 = 0, j0 = 0;
+      int e0 = 0;
 #pragma unroll
       for (int e = 0; e < VEC; ++e) {
         const float cc = __uint_as_float(__float_as_uint(cl[e]) ^ flip);
@@ -385,16 +390,40 @@ __global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
         if (a >= cut) {
           const int k = k0 + i, l = l0 + e;
           if (k < n - 1 && l > k && l < n) {
-            const double gk = __ldg(g64 + k), gl = __ldg(g64 + l);
-            const double wd = (double)w[i][e];
-            const bool agree = (((lw >> e) & 1u) == ((xk >> i) & 1u));
-            const double d = gk + gl - (agree ? 2.0 * wd : -2.0 * wd);
-            float v = (float)d;
+            float v;
+            if constexpr (sizeof(WT) == 1) {
+              // integer weights: every term is an integer below 2^24, so the
+              // fp32 estimate is the exact value
+              v = a;
+            } else {
+              const double gk = __ldg(g64 + k), gl = __ldg(g64 + l);
+              const double wd = (double)w[i][e];
+              const bool agree = (((lw >> e) & 1u) == ((xk >> i) & 1u));
+              v = (float)(gk + gl - (agree ? 2.0 * wd : -2.0 * wd));
+            }
+            const float vu = v;
             if (spin) v *= 2.0f;
+            if (!have_tj) {
+              // pair indices stay below 2^31 (n <= 46341)
+              const uint32_t c0 = (uint32_t)(pair_base(k, n) + (long long)(l - k - 1));
+              t0 = c0 % geo.G;
+              j0 = c0 / geo.G;
+              e0 = e;
+              have_tj = true;
+            }
+            uint32_t t = t0 + (uint32_t)(e - e0), j = j0;
+            while (t >= geo.G) {
+              t -= geo.G;
+              ++j;
+            }
+            const uint32_t grp = t / geo.L;
+            const uint32_t r = geo.rank[t - grp * geo.L];
             const uint64_t kk =
-                sel_key(v, (uint64_t)(pair_base(k, n) + (long long)(l - k - 1)), geo);
+                (r == 0xFFu || v != v)
+                    ? 0ull
+                    : (((uint64_t)ord_f32(v) << 32) |
+                       (uint64_t)(0xFFFFFFFFu - ((grp * geo.L + r) * geo.J + j)));
             best = kk > best ? kk : best;
-            const float vu = (float)d;
             if (kk != 0ull && vu > thr) {
               thr = vu;
               cut = thr - ldexpf(base + fabsf(thr), -20);
