@@ -684,6 +684,8 @@ def flip_bandwidth_leg(n=8192, tasks=1776, fields="auto"):
 #   cluster  a cluster ascent on SK n=8192 (8 starts, 8-CTA clusters), checked
 #            against the CTA-per-task form
 #   mpnn     one proposal-network forward and backward on G(16384, 0.01)
+#   csr      G(200000, 1e-4) N(0,1) on compressed rows: the sparse solver, the
+#            double pass and one descent
 # A leg exits non-zero when its result disagrees with its check.
 
 _flush_buf = None
@@ -930,7 +932,56 @@ def leg_mpnn(n=16384):
         raise SystemExit(1)
 
 
-LEGS = {"double": leg_double, "gray": leg_gray, "tfim": leg_tfim, "sparse": leg_sparse, "bnb": leg_bnb,
+def leg_csr(n=200000, p=1e-4):
+    """A sparse graph too large for the dense form, on compressed rows:
+    G(n, p) with N(0,1) weights (G(200000, 1e-4): 160 GB as a dense float32
+    matrix). spin_glass_solver_sparse from a random best_guess (host wall time,
+    rows built and uploaded inside), then the compressed-row double pass and
+    one descent timed alone (CUDA events)."""
+    import scipy.sparse as sp
+    import torch
+
+    from oracle import oracle as O
+    from pyqrackising_b200 import spin_glass_solver_sparse
+    from pyqrackising_b200.sparse import SparseDeviceGraph, use_compressed_rows
+
+    rng = np.random.default_rng(9)
+    m = int(n * (n - 1) / 2 * p)
+    r = rng.integers(0, n, size=2 * m)
+    c = rng.integers(0, n, size=2 * m)
+    keep = r < c
+    r, c = r[keep][:m], c[keep][:m]
+    U = sp.coo_matrix((rng.standard_normal(len(r)).astype(np.float32), (r, c)), shape=(n, n)).tocsr()
+    U.sum_duplicates()
+    guess = "".join("1" if b else "0" for b in rng.random(n) < 0.5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    bits, cut, _, energy = spin_glass_solver_sparse(U, best_guess=guess)
+    torch.cuda.synchronize()
+    t_solve = time.perf_counter() - t0
+    sg = SparseDeviceGraph(U)
+    words = sg.pack(np.array([b == "1" for b in bits]))
+    _, g64 = sg.gains(words)
+    G, L = O.flip_geometry(n, 148)
+    sg.double_bit_flips(words, g64, True, G, L)
+    ms_double = _timed(lambda: sg.double_bit_flips(words, g64, True, G, L), 3, flush=False)
+    start = sg.pack(rng.random(n) < 0.5)
+    _, gs = sg.gains(start)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    _, fl, rc = sg.single_descent(start, gs, True, G, L, 1 << 20)
+    b.record()
+    b.synchronize()
+    ms_desc = a.elapsed_time(b)
+    flips = int(fl.item())
+    _emit(leg="csr", graph=f"G({n}, {p}) N(0,1) float32", nnz=sg.nnz, dense_bytes=4 * n * n,
+          compressed_row_bytes=int(sg.nnz * 8 + (n + 1) * 8), uses_compressed_rows=use_compressed_rows(n),
+          solve_s=round(t_solve, 3), energy=energy, cut=cut,
+          double_pass_ms=round(ms_double, 3), pairs_per_s=n * (n - 1) / 2 / (ms_double / 1e3),
+          descent_ms=round(ms_desc, 2), descent_flips=flips, us_per_flip=round(1e3 * ms_desc / max(flips, 1), 3))
+
+
+LEGS = {"csr": leg_csr, "double": leg_double, "gray": leg_gray, "tfim": leg_tfim, "sparse": leg_sparse, "bnb": leg_bnb,
         "flips": leg_flips, "cluster": leg_cluster, "mpnn": leg_mpnn}
 
 
