@@ -126,11 +126,12 @@ __device__ __forceinline__ unsigned long long bmax_key(unsigned long long key) {
 // itself, so the next pass starts without a second barrier (a warp can be at
 // most one pass ahead of another, which writes the other slot array).
 // k < 0: no flip, only the selection. Returns the key and the exact gain of
-// the selected node. With float32 fields the pass also sums, in float64,
-// x_v W_kv over row k as it streams by: *out_gx = x_k sum_v x_v W_kv is then
-// the float64 gain of the flipped node k (its acceptance test and the running
-// value use it; the float32 fields only rank the candidates). The partial sums
-// ride on the same barrier as the selection.
+// the selected node. With float32 fields the pass also sums x_v W_kv over row
+// k as it streams by (per thread a compensated float pair, across threads in
+// float64): *out_gx = x_k sum_v x_v W_kv is then the gain of the flipped node
+// k to float64 accuracy (its acceptance test and the running value use it; the
+// float32 fields only rank the candidates). The partial sums ride on the same
+// barrier as the selection.
 template <typename WT, typename GT, int CH, bool STG, int BT>
 __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k, int xk,
                                                 unsigned long long (*red_key)[8],
@@ -138,7 +139,11 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
                                                 unsigned long long* out_key, double* out_g,
                                                 double* out_gx) {
   constexpr bool GX = std::is_same<GT, float>::value;
-  double px = 0.0;  // this thread's share of sum_v x_v W_kv (GX)
+  // this thread's share of sum_v x_v W_kv (GX) as an unevaluated float pair
+  // px_hi + px_lo: each term is added with an error-free two-sum, so the pair
+  // holds the sum to about 2^-47 of its magnitude without a float64
+  // conversion per term (those run on the slow conversion pipe)
+  float px_hi = 0.0f, px_lo = 0.0f;
   const int n = c.n;
   const GT coef = (k >= 0) ? (xk ? (GT)-2 : (GT)2) : (GT)0;
   const WT* __restrict__ row = c.W + (size_t)(k >= 0 ? k : 0) * c.ld;
@@ -170,7 +175,13 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
         const int xv = (word >> (v & 31)) & 1;
         if constexpr (GX) {
           // bit k may already be toggled here; W_kk = 0 in the prepared copy
-          if (k >= 0) px += xv ? (double)w4[i] : -(double)w4[i];
+          if (k >= 0) {
+            const float y = xv ? (float)w4[i] : -(float)w4[i];
+            const float t = px_hi + y;
+            const float bb = t - px_hi;
+            px_lo += (px_hi - (t - bb)) + (y - bb);
+            px_hi = t;
+          }
         }
         // v ascends within a thread: strict '>' keeps the lowest node
         if constexpr (std::is_same<GT, float>::value) {
@@ -270,6 +281,7 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   if (lane == 0) red_key[par][warp] = wk;
   if (key != 0ull && key == wk) red_g[par][warp] = bg;
   if constexpr (GX) {
+    double px = (double)px_hi + (double)px_lo;
     for (int o = 16; o > 0; o >>= 1) px += __shfl_xor_sync(0xFFFFFFFFu, px, o);
     if (lane == 0) red_x[par][warp] = px;
   }

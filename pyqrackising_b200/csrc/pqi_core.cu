@@ -4,6 +4,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <climits>
+#include <type_traits>
 
 #include "pqi_common.cuh"
 
@@ -297,65 +299,81 @@ __device__ __forceinline__ float thr_of(uint32_t o) {
   return o < ord_f32(-INFINITY) ? -INFINITY : unord_f32(o);
 }
 
+// The gains in the estimate's type, converted once per pass: float32 for float
+// weights, int32 (exact) for int8 weights.
+template <typename ET>
+__global__ void gains_to_estimate_kernel(const double* __restrict__ g64, int n, ET* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if constexpr (std::is_same<ET, float>::value) {
+      out[i] = (float)g64[i];
+    } else {
+      out[i] = (int)llrint(g64[i]);
+    }
+  }
+}
+
+// Tie priority of pair index c under the reference geometry, from (t, j) =
+// (c mod G, c / G); 32-bit (pair indices stay below 2^31 for n <= 46341).
+__device__ __forceinline__ uint64_t pair_key(float v, uint32_t t, uint32_t j, const SelGeom& geo) {
+  const uint32_t grp = t / geo.L;
+  const uint32_t r = geo.rank[t - grp * geo.L];
+  if (r == 0xFFu || v != v) return 0ull;
+  return ((uint64_t)ord_f32(v) << 32) | (uint64_t)(0xFFFFFFFFu - ((grp * geo.L + r) * geo.J + j));
+}
+
 template <typename WT>
 __global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
     const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
-    const double* __restrict__ g64, int spin, SelGeom geo, unsigned long long* key,
-    unsigned int* gthr) {
+    const double* __restrict__ g64, const void* __restrict__ gest_v, int spin, SelGeom geo,
+    unsigned long long* key, unsigned int* gthr) {
   constexpr int VEC = DoubleVec<WT>::VEC;
   constexpr int CW = VEC * DTHREADS;  // columns per tile
-  constexpr int BAND = CW / DR;       // row groups sharing one first column chunk
+  constexpr bool INT = sizeof(WT) == 1;
+  // the pair estimate's type: exact int32 for int8 weights, float32 otherwise
+  typedef typename std::conditional<INT, int, float>::type ET;
+  const ET* __restrict__ gest = static_cast<const ET*>(gest_v);
   __shared__ uint64_t scratch[32];
   __shared__ unsigned int s_thr;
   if (threadIdx.x == 0) s_thr = 0u;
   __syncthreads();
+  // tiles (row group rg, column chunk c) in a rectangle walked with a stride of
+  // gridDim.x, advanced without divisions; tiles wholly at or below the
+  // diagonal are skipped
   const int ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
   const int nc = (n + CW - 1) / CW;      // column chunks
-  const int nbands = (ng + BAND - 1) / BAND;
-  long long total = 0;
-  for (int b = 0; b < nbands; ++b)
-    total += (long long)(min(ng, (b + 1) * BAND) - b * BAND) * (nc - b);
+  const int dstep_rg = (int)(gridDim.x / nc), dstep_c = (int)(gridDim.x - (gridDim.x / nc) * nc);
+  int rg = (int)(blockIdx.x / nc), c = (int)(blockIdx.x - (blockIdx.x / nc) * nc);
   uint64_t best = 0;
   float thr = -INFINITY;
-  for (long long tau = blockIdx.x; tau < total; tau += gridDim.x) {
-    // tile tau -> (row group rg, column chunk c): band b holds row groups
-    // [b BAND, (b+1) BAND), each with chunks b .. nc-1 (chunks left of b lie
-    // wholly below the diagonal)
-    long long r = tau;
-    int b = 0;
-    while (true) {
-      const long long cnt = (long long)(min(ng, (b + 1) * BAND) - b * BAND) * (nc - b);
-      if (r < cnt) break;
-      r -= cnt;
-      ++b;
+  for (; rg < ng; rg += dstep_rg, c += dstep_c) {
+    if (c >= nc) {
+      c -= nc;
+      ++rg;
+      if (rg >= ng) break;
     }
-    const int per = nc - b;
-    const int rg = b * BAND + (int)(r / per);
-    const int c = b + (int)(r - (long long)(r / per) * per);
+    if ((c + 1) * CW <= rg * DR + 1) continue;  // every column <= every row's k
     const int k0 = rg * DR;
     const int l0 = c * CW + threadIdx.x * VEC;
     // the tile's rows: gains and bits (the same for every thread)
-    float fk[DR];
+    ET fk[DR];
     uint32_t xk = 0;
     float gt = 0.0f;
 #pragma unroll
     for (int i = 0; i < DR; ++i) {
       const int k = min(k0 + i, n - 1);
-      fk[i] = (float)__ldg(g64 + k);
-      gt = fmaxf(gt, fabsf(fk[i]));
+      fk[i] = __ldg(gest + k);
+      if constexpr (!INT) gt = fmaxf(gt, fabsf(fk[i]));
       xk |= (uint32_t)get_bit32(theta, k) << i;
     }
     // this thread's columns
-    float fl[VEC];
-    float cl[VEC];  // -2 where x_l = +1, +2 where x_l = -1
+    ET fl[VEC];
     float flmax = 0.0f;
     const uint32_t lw = l0 < n ? __ldg(theta + (l0 >> 5)) >> (l0 & 31) : 0u;
 #pragma unroll
     for (int e = 0; e < VEC; ++e) {
       const int l = l0 + e;
-      fl[e] = l < n ? (float)__ldg(g64 + l) : 0.0f;
-      flmax = fmaxf(flmax, fabsf(fl[e]));
-      cl[e] = ((lw >> e) & 1u) ? -2.0f : 2.0f;
+      fl[e] = l < n ? __ldg(gest + l) : ET(0);
+      if constexpr (!INT) flmax = fmaxf(flmax, fabsf(fl[e]));
     }
     // every row's W slice in flight before any is used (l0 < n keeps the
     // 16-byte load inside the padded row of ld >= n elements)
@@ -372,39 +390,49 @@ __global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
       }
     }
     thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(gthr))));
+    // the skip bound: 2^-20 (max |g_k| + max |g_l| + |thr|) for float
+    // estimates, none for exact integer ones
     const float base = gt + flmax;
-    float cut = thr - ldexpf(base + fabsf(thr), -20);
+    float cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
+    // integer estimates compare as integers (thr is then an integer value)
+    int cut_i = thr > -INFINITY ? (int)thr : INT_MIN;
 #pragma unroll
     for (int i = 0; i < DR; ++i) {
-      // c = -2 when bits k and l agree: cl already is for x_k = +1; x_k = -1 flips its sign
-      const uint32_t flip = (((xk >> i) & 1u) ^ 1u) << 31;
-      // (t, j) = (c mod G, c / G) of the first pair of the row that reaches the
-      // exact path (column e0), then advanced along the row's columns
+      const int xki = (xk >> i) & 1;
+      // (t, j) = (c mod G, c / G) of the first pair of the row that reaches
+      // the exact path (column e0), then advanced along the row's columns
       bool have_tj = false;
       uint32_t t0 = 0, j0 = 0;
       int e0 = 0;
 #pragma unroll
       for (int e = 0; e < VEC; ++e) {
-        const float cc = __uint_as_float(__float_as_uint(cl[e]) ^ flip);
-        const float a = fmaf(cc, (float)w[i][e], fk[i] + fl[e]);
-        if (a >= cut) {
+        // -2 W when bits k and l agree, +2 W otherwise
+        const bool agree = (((lw >> e) & 1u) == (uint32_t)xki);
+        float a = 0.0f;
+        int ai = 0;
+        bool pass;
+        if constexpr (INT) {
+          const int wi = (int)w[i][e];
+          ai = fk[i] + fl[e] + (agree ? -2 * wi : 2 * wi);  // the exact value
+          pass = ai >= cut_i;
+        } else {
+          a = fmaf(agree ? -2.0f : 2.0f, w[i][e], fk[i] + fl[e]);
+          pass = a >= cut;
+        }
+        if (pass) {
           const int k = k0 + i, l = l0 + e;
           if (k < n - 1 && l > k && l < n) {
             float v;
-            if constexpr (sizeof(WT) == 1) {
-              // integer weights: every term is an integer below 2^24, so the
-              // fp32 estimate is the exact value
-              v = a;
+            if constexpr (INT) {
+              v = (float)ai;  // below 2^24 in magnitude: exact
             } else {
               const double gk = __ldg(g64 + k), gl = __ldg(g64 + l);
               const double wd = (double)w[i][e];
-              const bool agree = (((lw >> e) & 1u) == ((xk >> i) & 1u));
               v = (float)(gk + gl - (agree ? 2.0 * wd : -2.0 * wd));
             }
             const float vu = v;
             if (spin) v *= 2.0f;
             if (!have_tj) {
-              // pair indices stay below 2^31 (n <= 46341)
               const uint32_t c0 = (uint32_t)(pair_base(k, n) + (long long)(l - k - 1));
               t0 = c0 % geo.G;
               j0 = c0 / geo.G;
@@ -416,17 +444,12 @@ __global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
               t -= geo.G;
               ++j;
             }
-            const uint32_t grp = t / geo.L;
-            const uint32_t r = geo.rank[t - grp * geo.L];
-            const uint64_t kk =
-                (r == 0xFFu || v != v)
-                    ? 0ull
-                    : (((uint64_t)ord_f32(v) << 32) |
-                       (uint64_t)(0xFFFFFFFFu - ((grp * geo.L + r) * geo.J + j)));
+            const uint64_t kk = pair_key(v, t, j, geo);
             best = kk > best ? kk : best;
             if (kk != 0ull && vu > thr) {
               thr = vu;
-              cut = thr - ldexpf(base + fabsf(thr), -20);
+              cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
+              cut_i = (int)thr;
             }
           }
         }
@@ -789,6 +812,15 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
   // key (8 bytes) and the shared threshold (4 bytes), zeroed together
   PQI_TRY(cudaMemsetAsync(key, 0, 16, s));
   unsigned int* gthr = reinterpret_cast<unsigned int*>(key + 1);
+  // the gains in the estimate's type (4 bytes each)
+  void* gest = ws.take<float>(n);
+  PQI_CHECK_ARG(gest);
+  if (w->kind == PQI_W_I8) {
+    gains_to_estimate_kernel<int><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(gains64, n, static_cast<int*>(gest));
+  } else {
+    gains_to_estimate_kernel<float><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(gains64, n, static_cast<float*>(gest));
+  }
+  PQI_LAUNCHED("gains_to_estimate_kernel");
   // one resident wave of blocks, persistent over the tiles
   static int resident[2] = {0, 0};
   const int i8 = w->kind == PQI_W_I8 ? 1 : 0;
@@ -801,10 +833,10 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     resident[i8] = std::max(1, sms * std::max(1, per_sm));
   }
   if (i8) {
-    double_tile_kernel<int8_t><<<resident[i8], DTHREADS, 0, s>>>(w->W_i8, w->ld, n, theta, gains64,
+    double_tile_kernel<int8_t><<<resident[i8], DTHREADS, 0, s>>>(w->W_i8, w->ld, n, theta, gains64, gest,
                                                                 is_spin_glass, geo, key, gthr);
   } else {
-    double_tile_kernel<float><<<resident[i8], DTHREADS, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64,
+    double_tile_kernel<float><<<resident[i8], DTHREADS, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64, gest,
                                                                is_spin_glass, geo, key, gthr);
   }
   PQI_LAUNCHED("double_tile_kernel");

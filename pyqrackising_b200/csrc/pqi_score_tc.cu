@@ -305,24 +305,31 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
     const int p = threadIdx.x - 192;
     constexpr int WPS = kInt8 ? 4 : 2;  // packed words per stage
     const int nstage = (t_end - t_begin) * kblocks;
-    const uint32_t ring = smem_u32(smem + NST * SB) + (uint32_t)p * 16u;
+    // ring slot layout [slot][word q][thread p]: a warp's copies of one word
+    // fall on 32 consecutive banks
+    const uint32_t ring = smem_u32(smem + NST * SB) + (uint32_t)p * 4u;
     // the stage being prefetched: tile ti, K block ki, ring slot si (all
     // advanced by one per issue, no divisions in the loop)
     int ti = t_begin, ki = 0, kp = 0, si = 0, issued = 0;
+    int tm_i = t_begin / ntn, tn_i = t_begin - (t_begin / ntn) * ntn;  // tile row / column of ti
     auto issue = [&]() {
       if (issued < nstage) {
-        const int b = (ti / ntn) * BM + p;
+        const int b = tm_i * BM + p;
         const int w0 = kp * (kInt8 ? 4 : 2);  // the stage's first word within the row
         const uint32_t* src = theta + (size_t)(b < shots ? b : 0) * n32;
         const uint32_t dst = ring + (uint32_t)si * (128u * 16u);
 #pragma unroll
         for (int q = 0; q < WPS; ++q)
-          cp_async4(dst + 4 * q, src + min(w0 + q, n32 - 1), b < shots && w0 + q < n32);
+          cp_async4(dst + 512u * q, src + min(w0 + q, n32 - 1), b < shots && w0 + q < n32);
         if (++kp == kb_per_pass) kp = 0;
         if (++ki == kblocks) {
           ki = 0;
           kp = 0;
           ++ti;
+          if (++tn_i == ntn) {
+            tn_i = 0;
+            ++tm_i;
+          }
         }
         ++issued;
       }
@@ -338,12 +345,12 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
     for (int st = 0; st < nstage; ++st) {
       cp_async_wait<PF - 1>();  // this stage's words have landed
       uint32_t wd[4];
-      const uint8_t* slot = smem + NST * SB + (size_t)p * 16 + (size_t)slot_i * (128 * 16);
+      const uint8_t* slot = smem + NST * SB + (size_t)p * 4 + (size_t)slot_i * (128 * 16);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) wd[q] = (q < WPS) ? *reinterpret_cast<const volatile uint32_t*>(slot + 4 * q) : 0u;
+      for (int q = 0; q < 4; ++q) wd[q] = (q < WPS) ? *reinterpret_cast<const volatile uint32_t*>(slot + 512 * q) : 0u;
       if (++slot_i == PF) slot_i = 0;
       issue();
-      if (st >= NST && !mbar_wait(&empty_bar[s], phase ^ 1u)) {
+      if (st >= NST && !mbar_wait_warp(&empty_bar[s], phase ^ 1u)) {
         ok = false;
         s_fail = 1;
       }
@@ -410,7 +417,7 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
       for (int pl = 0; pl < upt; ++pl, ++i) {
       const int a = i & 1;
       // columns beyond n hold zeros (TMA zero fill of W), so no column mask
-      const bool ready = mbar_wait(&accf_bar[a], (i >> 1) & 1);
+      const bool ready = mbar_wait_warp(&accf_bar[a], (i >> 1) & 1);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (__all_sync(0xFFFFFFFFu, ready)) {
         const uint32_t tbase =

@@ -43,22 +43,43 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                : "memory");
 }
 
-// Bounded wait for the phase with parity `parity`; false on timeout.
+// Bounded wait for the phase with parity `parity`; false on timeout. Each
+// try_wait may suspend the thread until the phase completes (hint: 0.1 ms),
+// and the clock is read once per 64 tries, so waiting threads leave the issue
+// slots and the clock pipe to the threads that work.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const uint32_t addr = smem_u32(bar);
-  const long long t0 = clock64();
-  while (true) {
+  long long t0 = 0;
+  for (uint32_t iter = 0;; ++iter) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.b32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
-        : "r"(addr), "r"(parity)
+        : "r"(addr), "r"(parity), "r"(100000u)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > WAIT_BUDGET_CYCLES) return false;
+    if ((iter & 63u) == 0u) {
+      const long long now = clock64();
+      if (iter == 0u) {
+        t0 = now;
+      } else if (now - t0 > WAIT_BUDGET_CYCLES) {
+        return false;
+      }
+    }
   }
+}
+
+// mbar_wait by lane 0 of the calling warp only; every lane gets the result.
+// The lanes' later shared-memory accesses are ordered after the wait by the
+// warp synchronisation.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity) {
+  bool ok = true;
+  if ((threadIdx.x & 31) == 0) ok = mbar_wait(bar, parity);
+  ok = __shfl_sync(0xFFFFFFFFu, ok ? 1 : 0, 0) != 0;
+  __syncwarp();
+  return ok;
 }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x,

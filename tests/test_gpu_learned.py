@@ -152,7 +152,8 @@ def test_kick_cdf_kernel():
     from pyqrackising_b200 import _lib
 
     rng = np.random.default_rng(3)
-    n, tasks, T, mix = 3001, 3, 2.5, 0.1
+    # (the kernel takes T and mix as float32: use values that float32 holds exactly)
+    n, tasks, T, mix = 3001, 3, 2.5, float(np.float32(0.1))
     z = rng.standard_normal((tasks, n)).astype(np.float32) * 4
     z[2, 17] = np.nan
     cdf = torch.empty(tasks * n, dtype=torch.float64, device="cuda")
