@@ -64,9 +64,10 @@ typedef struct {
   int ld;
   int kind;              /* pqi_wkind */
   double upper_sum;      /* sum_{u<v} W_uv (host value, filled by pqi_prepare_weights) */
-  const int8_t* W_d;     /* PQI_W_F32 (optional, pqi_prepare_digits): 3*n*ld int8, the
+  const int8_t* W_d;     /* PQI_W_F32 (optional, pqi_prepare_digits): 4*n*ld int8, the
                             fixed-point digit planes of W_f32z, else NULL */
-  double wscale;         /* W_f32z ~= wscale * (d0 2^16 + d1 2^8 + d2) (pqi_prepare_digits) */
+  double wscale;         /* W_f32z ~= wscale * (d0 2^24 + d1 2^16 + d2 2^8 + d3)
+                            (pqi_prepare_digits) */
 } pqi_weights;
 
 /* ---------------------------------------------------------------------------
@@ -122,10 +123,10 @@ pqi_status pqi_prepare_weights(const float* W, int n, const pqi_weight_stats* st
 
 /*
  * Fixed-point digit planes of float weights, for exact tensor-core scoring:
- * W_f32z times 2^S (S the largest integer with maxabs * 2^S < 2^22 - 1) is
- * rounded to integers v, |v| < 2^22, and split into balanced int8 digits,
- * v = d0 2^16 + d1 2^8 + d2 (d in [-128, 127]); planes d0, d1, d2 of n*ld bytes
- * each go to W_d (3*n*ld bytes). Fills w->W_d and w->wscale = 2^-S. The
+ * W_f32z times 2^S (S the largest integer with maxabs * 2^S < 2^30 - 1) is
+ * rounded to integers v, |v| < 2^30, and split into balanced int8 digits,
+ * v = d0 2^24 + d1 2^16 + d2 2^8 + d3 (d in [-128, 127]); planes d0..d3 of
+ * n*ld bytes each go to W_d (4*n*ld bytes). Fills w->W_d and w->wscale = 2^-S. The
  * scoring GEMM then accumulates each plane exactly in int32 and combines them
  * in 64-bit integers, so the only error of a score is the rounding of W to
  * multiples of 2^-S (at most 2^-S / 2 per weight). maxabs = max |W_ij| off the
@@ -135,12 +136,13 @@ pqi_status pqi_prepare_weights(const float* W, int n, const pqi_weight_stats* st
 pqi_status pqi_prepare_digits(pqi_weights* w, float maxabs, int8_t* W_d, void* stream);
 
 /* Select the batched-scoring implementation: 0 = tensor cores (tcgen05, the
- * default; the kernel expands the packed candidates into its +-1 operand
- * tiles itself; float weights as their int8 digit planes when prepared, with
- * exact integer accumulation), 1 = CUDA cores, 2 = tensor cores fed by a
- * separate expansion pass, 3 = as 2 with CTA pairs (cta_group::2 MMAs) for
- * batches of more than 128 candidates, 4 = as 0 but float weights as split
- * bf16 (hi + lo) with float32 accumulation. Process-wide; used to
+ * default; CTA pairs with cta_group::2 MMAs for batches of more than 128
+ * candidates, the +-1 operand expanded from the packed candidates by a
+ * separate pass; float weights as their int8 digit planes when prepared, with
+ * exact integer accumulation), 1 = CUDA cores, 2 = as 0 with single CTAs,
+ * 3 = as 0, 4 = as 0 but float weights as split bf16 (hi + lo) with float32
+ * accumulation, 5 = single CTAs that expand the packed candidates into their
+ * operand tiles themselves (no expansion pass). Process-wide; used to
  * cross-check the implementations. */
 pqi_status pqi_score_set_path(int path);
 

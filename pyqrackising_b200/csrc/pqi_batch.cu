@@ -388,13 +388,18 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
       }
     } else {
       // at most two groups per pass: eight accumulators keep the register
-      // budget of three resident CTAs per SM (one group with float64
-      // accumulators for float32 fields: four resident CTAs)
-      constexpr int CI = F32 ? 1 : (CH > 2 ? 2 : CH);
+      // budget of three resident CTAs per SM. Float32 fields sum each field
+      // as an unevaluated float pair (error-free two-sum per term: float32
+      // adds only, no float64 conversion per term), so the field and the
+      // starting value are float64-accurate.
+      constexpr int CI = F32 ? 1 : (CH > 2 ? 2 : CH);  // (float pairs: one group)
       for (int base = 4 * threadIdx.x; base < n; base += CI * 4 * BT) {
-        AT acc[4 * CI];
+        GT acc[4 * CI];
+        float alo[F32 ? 4 * CI : 1];
 #pragma unroll
         for (int e = 0; e < 4 * CI; ++e) acc[e] = 0;
+#pragma unroll
+        for (int e = 0; e < (F32 ? 4 * CI : 1); ++e) alo[e] = 0.0f;
 #pragma unroll 2
         for (int u = 0; u < n; ++u) {
           const WT* __restrict__ row = c.W + (size_t)u * c.ld;
@@ -417,7 +422,17 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
                 for (int i = 0; i < 4; ++i) w4[i] = (v + i < n) ? __ldg(row + v + i) : (WT)0;
               }
 #pragma unroll
-              for (int i = 0; i < 4; ++i) acc[4 * j + i] += xu ? (AT)w4[i] : -(AT)w4[i];
+              for (int i = 0; i < 4; ++i) {
+                if constexpr (F32) {
+                  const float y = xu ? (float)w4[i] : -(float)w4[i];
+                  const float t = acc[4 * j + i] + y;
+                  const float bb = t - acc[4 * j + i];
+                  alo[4 * j + i] += (acc[4 * j + i] - (t - bb)) + (y - bb);
+                  acc[4 * j + i] = t;
+                } else {
+                  acc[4 * j + i] += xu ? (GT)w4[i] : -(GT)w4[i];
+                }
+              }
             }
           }
         }
@@ -426,7 +441,11 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             const int v = base + j * 4 * BT + i;
-            if (v < n) store_field(v, acc[4 * j + i]);
+            if constexpr (F32) {
+              if (v < n) store_field(v, (double)acc[4 * j + i] + (double)alo[4 * j + i]);
+            } else {
+              if (v < n) store_field(v, acc[4 * j + i]);
+            }
           }
       }
     }

@@ -163,20 +163,20 @@ __global__ void prep_convert_kernel(const float* __restrict__ W, int n, int ld,
   }
 }
 
-// Fixed-point digit planes: v = rint(w * 2^S), |v| < 2^22, balanced int8
-// digits v = d0 2^16 + d1 2^8 + d2 into three planes of n*ld bytes.
+// Fixed-point digit planes: v = rint(w * 2^S), |v| < 2^30, balanced int8
+// digits v = d0 2^24 + d1 2^16 + d2 2^8 + d3 into four planes of n*ld bytes.
 __global__ void prep_digits_kernel(const float* __restrict__ Wz, size_t total, double scale,
                                    int8_t* __restrict__ Wd) {
   for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (size_t)gridDim.x * blockDim.x) {
-    const long long v = llrint((double)Wz[e] * scale);
-    const int d2 = (int)(((v + 128) & 255) - 128);
-    const long long v1 = (v - d2) / 256;
-    const int d1 = (int)(((v1 + 128) & 255) - 128);
-    const int d0 = (int)((v1 - d1) / 256);
-    Wd[e] = (int8_t)d0;
-    Wd[total + e] = (int8_t)d1;
-    Wd[2 * total + e] = (int8_t)d2;
+    long long v = llrint((double)Wz[e] * scale);
+#pragma unroll
+    for (int p = 3; p > 0; --p) {
+      const int d = (int)(((v + 128) & 255) - 128);
+      Wd[(size_t)p * total + e] = (int8_t)d;
+      v = (v - d) / 256;
+    }
+    Wd[e] = (int8_t)v;  // |v| <= 64 here
   }
 }
 
@@ -715,14 +715,15 @@ pqi_status pqi_prepare_weights(const float* W, int n, const pqi_weight_stats* st
 pqi_status pqi_prepare_digits(pqi_weights* w, float maxabs, int8_t* W_d, void* stream) {
   PQI_CHECK_ARG(w && W_d && w->W_f32z && w->kind == PQI_W_F32 && w->n > 0 && maxabs >= 0.0f &&
                 std::isfinite(maxabs));
-  // largest S with maxabs * 2^S < 2^22 - 1 (rounding then stays below 2^22)
+  // largest S with maxabs * 2^S < 2^30 - 1 (rounding then stays below 2^30)
+  const double lim = 1073741823.0;
   int S = 0;
   if (maxabs > 0.0f) {
     int e = 0;
     std::frexp((double)maxabs, &e);  // maxabs = f 2^e, f in [0.5, 1)
-    S = 21 - e;                       // maxabs 2^S < 2^21
-    while (std::ldexp((double)maxabs, S + 1) < 4194303.0) ++S;
-    while (std::ldexp((double)maxabs, S) >= 4194303.0) --S;
+    S = 29 - e;                       // maxabs 2^S < 2^29
+    while (std::ldexp((double)maxabs, S + 1) < lim) ++S;
+    while (std::ldexp((double)maxabs, S) >= lim) --S;
   }
   const size_t total = (size_t)w->n * w->ld;
   prep_digits_kernel<<<grid_for((long long)total, 256, 148 * 16), 256, 0, as_stream(stream)>>>(

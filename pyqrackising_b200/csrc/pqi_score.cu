@@ -148,10 +148,11 @@ pqi_status score_simt(const pqi_weights* w, const uint32_t* theta, int shots, do
   return PQI_OK;
 }
 
-// Set by pqi_score_set_path: 0 = automatic (tensor cores when available, the
-// A operand expanded inside the scoring kernel), 1 = CUDA cores only,
-// 2 = tensor cores with a separate expansion pass, 3 = as 2 with CTA pairs,
-// 4 = as 0 with float weights as split bf16. Used by tests to compare the paths.
+// Set by pqi_score_set_path: 0 = automatic (tensor cores when available, CTA
+// pairs fed by a separate expansion pass), 1 = CUDA cores only, 2 = single
+// CTAs, 3 = CTA pairs (as 0), 4 = as 0 with float weights as split bf16,
+// 5 = single CTAs that expand the candidates themselves. Used by tests to
+// compare the paths.
 int g_score_path = 0;
 
 pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int spin,
@@ -172,7 +173,7 @@ using namespace pqi;
 extern "C" {
 
 pqi_status pqi_score_set_path(int path) {
-  if (path < 0 || path > 4) return PQI_EINVAL;
+  if (path < 0 || path > 5) return PQI_EINVAL;
   g_score_path = path;
   return PQI_OK;
 }

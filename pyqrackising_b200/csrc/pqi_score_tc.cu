@@ -123,7 +123,8 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
     score_tc_kernel(const __grid_constant__ CUtensorMap map_a,
                     const __grid_constant__ CUtensorMap map_b0,
                     const __grid_constant__ CUtensorMap map_b1,
-                    const __grid_constant__ CUtensorMap map_b2, int planes, double qscale,
+                    const __grid_constant__ CUtensorMap map_b2,
+                    const __grid_constant__ CUtensorMap map_b3, int planes, double qscale,
                     int n, int shots,
                     const uint32_t* __restrict__ theta, int n32, double upper_sum, int spin,
                     SelGeom geo, double* __restrict__ qpart, float* __restrict__ energies,
@@ -160,7 +161,7 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
   const int t_begin = (int)(((long long)unit * ntiles) / units);
   const int t_end = (int)(((long long)(unit + 1) * ntiles) / units);
   const int kb_per_pass = kInt8 ? (n + BK_BYTES - 1) / BK_BYTES : (n + 63) / 64;
-  // int8 operands: `planes` K passes, each its own accumulation (planes = 3:
+  // int8 operands: `planes` K passes, each its own accumulation (planes = 4:
   // the digit planes of float weights, combined exactly in the epilogue);
   // bf16: the hi and lo passes accumulate into one accumulator
   const int upt = kInt8 ? planes : 1;                       // accumulations per tile
@@ -219,7 +220,8 @@ __global__ void __launch_bounds__(FUSED ? FTHREADS : PTHREADS, 1)
             break;
           }
           const int kk = kInt8 ? kp * BK_BYTES : kp * 64;
-          const CUtensorMap* mb = pass == 0 ? &map_b0 : (pass == 1 ? &map_b1 : &map_b2);
+          const CUtensorMap* mb =
+              pass == 0 ? &map_b0 : (pass == 1 ? &map_b1 : (pass == 2 ? &map_b2 : &map_b3));
           if (++kp == kb_per_pass) {
             kp = 0;
             ++pass;
@@ -712,21 +714,22 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
   if (!arch_ok || !encode_fn()) return PQI_ENOTSUP;
   const int n = w->n, n32 = (n + 31) >> 5, ld = w->ld;
   // int8 tensor-core operands: integer weights (one plane), or float weights
-  // as three fixed-point digit planes (exact integer sums, scaled by wscale);
+  // as four fixed-point digit planes (exact integer sums, scaled by wscale);
   // path 4 scores float weights as split bf16 instead
   const bool digits = w->kind != PQI_W_I8 && w->W_d && g_score_path != 4;
   const bool i8 = w->kind == PQI_W_I8 || digits;
-  const int planes = digits ? 3 : 1;
+  const int planes = digits ? 4 : 1;
   const double qscale = digits ? w->wscale : 1.0;
   // the int8 epilogue sums 256 columns of |Y| <= 127 n in 32 bits
   if (i8 && n > 65536) return PQI_ENOTSUP;
   const int ntn = (n + tc::BN - 1) / tc::BN;
   const int ntm = (shots + tc::BM - 1) / tc::BM;
-  // 0 (default): single CTAs that expand the packed candidates into the A
-  // tiles themselves; 2: single CTAs, A expanded by a separate pass and loaded
-  // by TMA; 3: CTA pairs (cta_group::2), A as in 2
-  const bool fused = g_score_path == 0 || g_score_path == 4;
-  const bool pair = g_score_path == 3 && ntm >= 2;
+  // 0 (default), 3 and 4: CTA pairs (cta_group::2) for more than 128
+  // candidates, the A operand expanded by a separate pass and loaded by TMA;
+  // 2: single CTAs, A as in 0; 5: single CTAs that expand the packed
+  // candidates into the A tiles themselves
+  const bool fused = g_score_path == 5;
+  const bool pair = g_score_path != 2 && !fused && ntm >= 2;
   // one zeroed control block: err, mdone, key, then mcount[ntm]
   const size_t ctl_bytes = 64 + (size_t)ntm * sizeof(unsigned);
   uint8_t* ctl = ws.take<uint8_t>(ctl_bytes);
@@ -745,16 +748,18 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     return PQI_EINVAL;
   }
   const int brows = pair ? tc::BN / 2 : tc::BN;
-  // the B operand's maps: int8 weights (all three the same), digit planes
-  // 0..2 (n*ld bytes apart), or bf16 hi and lo
+  // the B operand's maps: int8 weights (all the same), digit planes 0..3
+  // (n*ld bytes apart), or bf16 hi and lo
   const size_t plane_bytes = (size_t)n * ld;
   const void* b0 = digits ? (const void*)w->W_d : (i8 ? (const void*)w->W_i8 : (const void*)w->W_hi);
   const void* b1 = digits ? (const void*)(w->W_d + plane_bytes) : (i8 ? b0 : (const void*)w->W_lo);
   const void* b2 = digits ? (const void*)(w->W_d + 2 * plane_bytes) : b1;
-  CUtensorMap ma, mb0, mb1, mb2;
+  const void* b3 = digits ? (const void*)(w->W_d + 3 * plane_bytes) : b2;
+  CUtensorMap ma, mb0, mb1, mb2, mb3;
   if (!cached_map(&mb0, b0, i8, n, n, ld, brows)) return PQI_ENOTSUP;
   if (!cached_map(&mb1, b1, i8, n, n, ld, brows)) return PQI_ENOTSUP;
   if (!cached_map(&mb2, b2, i8, n, n, ld, brows)) return PQI_ENOTSUP;
+  if (!cached_map(&mb3, b3, i8, n, n, ld, brows)) return PQI_ENOTSUP;
   if (fused) {
     ma = mb0;  // not read: the kernel writes its A tiles itself
   } else if (!cached_map(&ma, X, i8, shots, n, ld, tc::BM)) {
@@ -811,11 +816,11 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     const int pairs = std::max(1, std::min({tiles, limit / 2, fit[i8]}));
     cfg.gridDim = dim3(2 * pairs);
     if (i8) {
-      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<true, true, false>, ma, mb0, mb1, mb2, planes, qscale, n, shots,
+      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<true, true, false>, ma, mb0, mb1, mb2, mb3, planes, qscale, n, shots,
                                  theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
                                  mdone, key, best_energy, best_index, err));
     } else {
-      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<false, true, false>, ma, mb0, mb1, mb2, planes, qscale, n, shots,
+      PQI_TRY(cudaLaunchKernelEx(&cfg, tc::score_tc_kernel<false, true, false>, ma, mb0, mb1, mb2, mb3, planes, qscale, n, shots,
                                  theta, n32, w->upper_sum, spin, geo, qpart, energies, mcount,
                                  mdone, key, best_energy, best_index, err));
     }
@@ -824,12 +829,12 @@ pqi_status score_tc(const pqi_weights* w, const uint32_t* theta, int shots, int 
     const int threads = fused ? tc::FTHREADS : tc::PTHREADS;
     if (i8) {
       auto k = fused ? tc::score_tc_kernel<true, false, true> : tc::score_tc_kernel<true, false, false>;
-      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, mb2, planes, qscale, n, shots, theta, n32, w->upper_sum, spin, geo,
+      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, mb2, mb3, planes, qscale, n, shots, theta, n32, w->upper_sum, spin, geo,
                                           qpart, energies, mcount, mdone, key, best_energy, best_index,
                                           err);
     } else {
       auto k = fused ? tc::score_tc_kernel<false, false, true> : tc::score_tc_kernel<false, false, false>;
-      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, mb2, planes, qscale, n, shots, theta, n32, w->upper_sum, spin, geo,
+      k<<<grid, threads, smem_bytes, s>>>(ma, mb0, mb1, mb2, mb3, planes, qscale, n, shots, theta, n32, w->upper_sum, spin, geo,
                                           qpart, energies, mcount, mdone, key, best_energy, best_index,
                                           err);
     }

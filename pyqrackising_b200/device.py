@@ -10,7 +10,7 @@ HBM layout per graph of n nodes (ld = n rounded up to 128):
   W_f32z  n*ld  float32   zero diagonal, zero padding
   W_i8    n*ld  int8      integer weights in [-127, 127] (else absent)
   W_hi/lo n*ld  bf16 x2   split of float weights (else absent)
-  W_d     3*n*ld int8    fixed-point digit planes of float weights (else absent)
+  W_d     4*n*ld int8    fixed-point digit planes of float weights (else absent)
 """
 
 from __future__ import annotations
@@ -157,7 +157,7 @@ class DeviceGraph:
         self.W_d = None
         if st.kind != _lib.PQI_W_I8:
             # float weights: also their fixed-point digit planes (exact scoring)
-            self.W_d = torch.empty(3 * n * ld, dtype=torch.int8, device=self.device)
+            self.W_d = torch.empty(4 * n * ld, dtype=torch.int8, device=self.device)
             call("pqi_prepare_digits", ctypes.byref(self.w), ctypes.c_float(st.maxabs), _ptr(self.W_d), self.sp())
         self.n32 = (n + 31) >> 5
         self.n64 = (n + 63) >> 6

@@ -104,7 +104,7 @@ def test_double_flips(name, oracle_mod):
 
 
 @pytest.mark.parametrize("name", NAMES)
-@pytest.mark.parametrize("path", [0, 1, 3])
+@pytest.mark.parametrize("path", [0, 1, 2, 5])
 def test_calculate_cut(name, path, oracle_mod):
     from pyqrackising_b200 import _lib
 

@@ -47,12 +47,11 @@ def test_tensor_core_scoring(n, shots, kind, oracle_mod):
         else:
             tol = 1e-5 * np.abs(W.astype(np.float64)).sum() / 2
             assert np.all(np.abs(got - exact) <= tol), np.abs(got - exact).max() / tol
-        # same answer from the CUDA-core path (1), the tensor-core paths fed by
-        # a separate expansion pass, single CTAs (2) and CTA pairs (3), and the
-        # split-bf16 form of float weights (4); the default (0) expands the
-        # candidates inside the scoring kernel and scores float weights as
-        # fixed-point digit planes
-        for path in (1, 2, 3, 4):
+        # same answer from the CUDA-core path (1), single CTAs (2), CTA pairs
+        # (3, the default's form), the split-bf16 form of float weights (4) and
+        # single CTAs that expand the candidates themselves (5); the default
+        # (0) scores float weights as fixed-point digit planes
+        for path in (1, 2, 3, 4, 5):
             _lib.call("pqi_score_set_path", path)
             try:
                 e1, be1, bi1 = dg.calculate_cut(words, shots, spin, G, L)
