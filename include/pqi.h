@@ -639,6 +639,20 @@ pqi_status pqi_csr_double_bit_flips(const pqi_csr* g, const uint32_t* theta, con
                                     float* best_energy, long long* best_index, void* workspace,
                                     size_t workspace_bytes, void* stream);
 
+/* pqi_csr_double_bit_flips for a caller that applies the selected pair only
+ * when its value is > 0 (the solver loop, spin_glass_solver_sparse.py:727-751):
+ * whenever the best pair value is > 0, the same best_energy and best_index;
+ * otherwise best_energy <= 0 (-inf allowed) and best_index is -1 or a pair of
+ * that value. Pairs whose fp32 estimate is not > 0 are never scored, so at a
+ * single-flip local optimum (every gain <= 0) only the adjacent pairs are.
+ * Same arguments and workspace. No reference counterpart (an early-out of the
+ * reference's own loop). */
+pqi_status pqi_csr_improving_double_flip(const pqi_csr* g, const uint32_t* theta,
+                                         const double* gains64, int is_spin_glass,
+                                         int global_size, int local_size, float* best_energy,
+                                         long long* best_index, void* workspace,
+                                         size_t workspace_bytes, void* stream);
+
 /* pqi_gray on CSR (the gray_sparse kernel's schedule, kernels.cl:1072-1150);
  * gains64 required. Workspace: n float64 per resident seed. */
 pqi_status pqi_csr_gray(const pqi_csr* g, const uint64_t* theta64, const double* gains64,

@@ -151,6 +151,7 @@ SIGNATURES = {
     "pqi_csr_apply_flip": (_i, [_CP, _vp, _vp, _i, _i, _vp]),
     "pqi_csr_single_descent": (_i, [_CP, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _sz, _vp]),
     "pqi_csr_double_bit_flips": (_i, [_CP, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _sz, _vp]),
+    "pqi_csr_improving_double_flip": (_i, [_CP, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_csr_gray": (_i, [_CP, _vp, _vp, _i, ctypes.c_longlong, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_csr_rescore_fp64": (_i, [_CP, _vp, _i, _vp, _vp, _vp]),
     "pqi_csr_calculate_cut": (_i, [_CP, _vp, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _sz, _vp]),

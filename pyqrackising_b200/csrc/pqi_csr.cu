@@ -76,35 +76,60 @@ __device__ __forceinline__ void block_flip(double* g, W* bits, const long long* 
 // Single CTA: repeat (best single flip under the reference geometry, flip it
 // if its value is > 0) until none improves or max_flips is reached
 // (spin_glass_solver_sparse.py:703-726, repeated).
+//
+// The nodes are cut into segments of `seg` nodes whose largest selection key
+// stays in shared memory. A flip changes only the gains of the flipped node
+// and its neighbours, so after it only their segments are rescanned (a warp
+// per segment) and the next selection is a maximum over the segment keys:
+// per flip O(degree * seg + n / seg) work instead of a pass over all n gains.
+// The selected key is the same maximum over all nodes' keys.
+__device__ __forceinline__ uint64_t segment_key(const double* __restrict__ g, int n, int seg, int q,
+                                                int spin, const SelGeom& geo) {
+  uint64_t best = 0;
+  float bv = -INFINITY;
+  const int k1 = min(n, (q + 1) * seg);
+  for (int k = q * seg + (threadIdx.x & 31); k < k1; k += 32) {
+    float v = (float)__ldcg(g + k);
+    if (spin) v *= 2.0f;
+    if (v >= bv) {  // a smaller value cannot give a larger key
+      const uint64_t kk = sel_key(v, (uint64_t)k, geo);
+      if (kk > best) {
+        best = kk;
+        bv = v;
+      }
+    }
+  }
+  return warp_max_u64(best);
+}
+
 __global__ void __launch_bounds__(1024) descent_kernel(
     const long long* __restrict__ ptr, const int* __restrict__ col, const float* __restrict__ val,
-    int n, uint32_t* __restrict__ theta, double* __restrict__ g, int spin, SelGeom geo,
+    int n, int seg, uint32_t* __restrict__ theta, double* __restrict__ g, int spin, SelGeom geo,
     int max_flips, double* __restrict__ energy_sum, int* __restrict__ flips,
     int* __restrict__ trace, int* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint64_t scratch[32];
+  __shared__ int s_count;
   const int n32 = (n + 31) >> 5;
-  uint32_t* bits = reinterpret_cast<uint32_t*>(smem);
+  const int nseg = (n + seg - 1) / seg;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  uint64_t* skey = reinterpret_cast<uint64_t*>(smem);
+  int* list = reinterpret_cast<int*>(skey + nseg);
+  uint8_t* dirty = reinterpret_cast<uint8_t*>(list + nseg);
+  uint32_t* bits = reinterpret_cast<uint32_t*>(smem + (((size_t)nseg * 13 + 15) & ~size_t(15)));
   for (int q = threadIdx.x; q < n32; q += blockDim.x) bits[q] = theta[q];
+  for (int q = threadIdx.x; q < nseg; q += blockDim.x) dirty[q] = 0;
+  for (int q = warp; q < nseg; q += nwarps) {
+    const uint64_t kq = segment_key(g, n, seg, q, spin, geo);
+    if (lane == 0) skey[q] = kq;
+  }
+  if (threadIdx.x == 0) s_count = 0;
   __syncthreads();
   double esum = 0.0;
   int cnt = 0, st = PQI_OK;
   while (true) {
-    // a value below the thread's best so far cannot give a larger key: the
-    // key (and its divisions) only for candidates that reach it
     uint64_t best = 0;
-    float bv = -INFINITY;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      float v = (float)g[k];
-      if (spin) v *= 2.0f;
-      if (v >= bv) {
-        const uint64_t kk = sel_key(v, (uint64_t)k, geo);
-        if (kk > best) {
-          best = kk;
-          bv = v;
-        }
-      }
-    }
+    for (int q = threadIdx.x; q < nseg; q += blockDim.x) best = skey[q] > best ? skey[q] : best;
     best = block_max_u64(best, scratch);
     float v;
     int64_t idx;
@@ -117,7 +142,36 @@ __global__ void __launch_bounds__(1024) descent_kernel(
     esum += (double)v;
     if (threadIdx.x == 0 && trace) trace[cnt] = (int)idx;
     ++cnt;
-    block_flip<uint32_t>(g, bits, ptr, col, val, (int)idx);
+    // the flip, marking the segments whose gains change
+    const int k = (int)idx;
+    const int xk = bit_at(bits, k);
+    if (threadIdx.x == 0) dirty[k / seg] = 1;
+    for (long long e = ptr[k] + threadIdx.x; e < ptr[k + 1]; e += blockDim.x) {
+      const int u = __ldg(col + e);
+      const double w2 = 2.0 * (double)__ldg(val + e);
+      g[u] += (bit_at(bits, u) == xk) ? -w2 : w2;
+      dirty[u / seg] = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // after the row's updates (as block_flip)
+      g[k] = -g[k];
+      bits[k >> 5] ^= 1u << (k & 31);
+    }
+    for (int q = threadIdx.x; q < nseg; q += blockDim.x) {
+      if (dirty[q]) {
+        dirty[q] = 0;
+        list[atomicAdd(&s_count, 1)] = q;
+      }
+    }
+    __syncthreads();
+    const int nd = s_count;
+    for (int i = warp; i < nd; i += nwarps) {
+      const int q = list[i];
+      const uint64_t kq = segment_key(g, n, seg, q, spin, geo);
+      if (lane == 0) skey[q] = kq;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_count = 0;
   }
   for (int q = threadIdx.x; q < n32; q += blockDim.x) theta[q] = bits[q];
   if (threadIdx.x == 0) {
@@ -349,6 +403,10 @@ struct PairState {
   unsigned int* vmax;          // ordered float32 of the maximum (phase 1 result)
   unsigned long long* prio;    // smallest priority at the maximum (phase 2)
   unsigned int* thr;           // phase 1: shared threshold (ordered, unscaled value)
+  unsigned int* bound;         // ordered: [0] max f_k, [1] max |f_k|, then the row
+                               // groups' max f_k ([2, 2 + ng)), then the column
+                               // chunks' max f_k ([2 + ng, 2 + ng + nc))
+  int positive;                // only pairs of value > 0 are wanted
 };
 
 __device__ __forceinline__ float thr_of(uint32_t o) {
@@ -414,6 +472,11 @@ __global__ void pair_edges_kernel(const long long* __restrict__ ptr, const int* 
 }
 
 // All pairs in tiles of DR rows x CW columns (the upper triangle), gains only.
+// The float32 gains f_k are rounded up from the float64 gains (f_k >= g_k), so
+// the fp32 estimate of a non-adjacent pair is > 0 whenever its value is, and
+// the largest f_k of a row group plus that of a column chunk bounds every
+// estimate of their tile: a row group or a tile whose bound is below the cut
+// is passed over without loading its gains.
 template <int PHASE>
 __global__ void __launch_bounds__(DT) pair_tiles_kernel(
     const long long* __restrict__ ptr, const int* __restrict__ col, const float* __restrict__ val,
@@ -422,74 +485,85 @@ __global__ void __launch_bounds__(DT) pair_tiles_kernel(
   __shared__ unsigned int s_thr;
   if (threadIdx.x == 0) s_thr = 0u;
   __syncthreads();
-  // tiles (row group rg, column chunk c) in a rectangle; those wholly at or
-  // below the diagonal are skipped
   const int ng = (n - 1 + DR - 1) / DR;
   const int nc = (n + CW - 1) / CW;
-  const long long total = (long long)ng * nc;
   unsigned int best_o = 0;
   unsigned long long best_p = ~0ull;
   // phase 2 looks for the pairs whose scaled value is vmax
   const unsigned int target = PHASE == 2 ? *ps.vmax : 0u;
   const float vt = PHASE == 2 ? thr_of(target) : 0.0f;
+  if (PHASE == 2 && (target == 0u || (ps.positive && !(vt > 0.0f)))) return;
+  // positive: an estimate must be > 0 (>= the smallest positive float)
+  const float floor_cut = ps.positive ? __int_as_float(1) : -INFINITY;
+  const float gmax = thr_of(ps.bound[0]);
+  const float gabs = thr_of(ps.bound[1]);
+  const unsigned int* rgmax = ps.bound + 2;
+  const unsigned int* cmax = rgmax + ng;
   float thr = PHASE == 2 ? (spin ? vt * 0.5f : vt) : -INFINITY;
-  for (long long tau = blockIdx.x; tau < total; tau += gridDim.x) {
-    const int rg = (int)(tau / nc);
-    const int c = (int)(tau - (long long)rg * nc);
-    if ((c + 1) * CW <= rg * DR + 1) continue;  // every column <= every row's k
+  for (int rg = blockIdx.x; rg < ng; rg += gridDim.x) {
     const int k0 = rg * DR;
-    const int l0 = c * CW + threadIdx.x * VEC;
-    float fk[DR];
-    float gt = 0.0f;
-#pragma unroll
-    for (int i = 0; i < DR; ++i) {
-      fk[i] = __ldg(g32 + min(k0 + i, n - 1));
-      gt = fmaxf(gt, fabsf(fk[i]));
-    }
-    float fl[VEC];
-    float flmax = 0.0f;
-#pragma unroll
-    for (int e = 0; e < VEC; ++e) {
-      fl[e] = (l0 + e < n) ? __ldg(g32 + l0 + e) : -INFINITY;
-      if (l0 + e < n) flmax = fmaxf(flmax, fabsf(fl[e]));
-    }
+    const float rmax = thr_of(__ldg(rgmax + rg));
     if (PHASE == 1) thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(ps.thr))));
-    const float base = gt + flmax;
-    float cut = thr - ldexpf(base + fabsf(thr), -20);
+    // (a cut at least as low as every tile's: its base bounds every base below)
+    const float row_cut = fmaxf(thr - ldexpf(2.0f * gabs + fabsf(thr), -20), floor_cut);
+    if (!(rmax + gmax >= row_cut)) continue;
+    // the first column chunk with a column above the group's first row
+    for (int c = (k0 + 1) / CW; c < nc; ++c) {
+      if (PHASE == 1) thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(ps.thr))));
+      const float tile_cut = fmaxf(thr - ldexpf(2.0f * gabs + fabsf(thr), -20), floor_cut);
+      if (!(rmax + thr_of(__ldg(cmax + c)) >= tile_cut)) continue;
+      const int l0 = c * CW + threadIdx.x * VEC;
+      float fk[DR];
+      float gt = 0.0f;
 #pragma unroll
-    for (int i = 0; i < DR; ++i) {
+      for (int i = 0; i < DR; ++i) {
+        fk[i] = __ldg(g32 + min(k0 + i, n - 1));
+        gt = fmaxf(gt, fabsf(fk[i]));
+      }
+      float fl[VEC];
+      float flmax = 0.0f;
 #pragma unroll
       for (int e = 0; e < VEC; ++e) {
-        const float a = fk[i] + fl[e];
-        if (a >= cut) {
-          const int k = k0 + i, l = l0 + e;
-          if (k < n - 1 && l > k && l < n) {
-            float vu, vs;
-            pair_value(__ldg(g64 + k), __ldg(g64 + l), weight_of(ptr, col, val, k, l),
-                       bit_at(theta, k), bit_at(theta, l), spin, &vu, &vs);
-            const unsigned long long pr =
-                pair_prio((unsigned long long)pair_index(k, l, n), geo);
-            if (pr != ~0ull && vs == vs) {
-              const unsigned int o = ord_f32(vs);
-              if (PHASE == 1) {
-                best_o = o > best_o ? o : best_o;
-                if (vu > thr) {
-                  thr = vu;
-                  cut = thr - ldexpf(base + fabsf(thr), -20);
+        fl[e] = (l0 + e < n) ? __ldg(g32 + l0 + e) : -INFINITY;
+        if (l0 + e < n) flmax = fmaxf(flmax, fabsf(fl[e]));
+      }
+      const float base = gt + flmax;
+      float cut = fmaxf(thr - ldexpf(base + fabsf(thr), -20), floor_cut);
+#pragma unroll
+      for (int i = 0; i < DR; ++i) {
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) {
+          const float a = fk[i] + fl[e];
+          if (a >= cut) {
+            const int k = k0 + i, l = l0 + e;
+            if (k < n - 1 && l > k && l < n) {
+              float vu, vs;
+              pair_value(__ldg(g64 + k), __ldg(g64 + l), weight_of(ptr, col, val, k, l),
+                         bit_at(theta, k), bit_at(theta, l), spin, &vu, &vs);
+              const unsigned long long pr =
+                  pair_prio((unsigned long long)pair_index(k, l, n), geo);
+              if (pr != ~0ull && vs == vs) {
+                const unsigned int o = ord_f32(vs);
+                if (PHASE == 1) {
+                  best_o = o > best_o ? o : best_o;
+                  if (vu > thr) {
+                    thr = vu;
+                    cut = fmaxf(thr - ldexpf(base + fabsf(thr), -20), floor_cut);
+                  }
+                } else if (o == target && pr < best_p) {
+                  best_p = pr;
                 }
-              } else if (o == target && pr < best_p) {
-                best_p = pr;
               }
             }
           }
         }
       }
-    }
-    if (PHASE == 1 && thr > -INFINITY) {
-      const unsigned int o = ord_f32(thr);
-      if (o > *(volatile unsigned int*)&s_thr) {
-        atomicMax(&s_thr, o);
-        if (o > __ldcg(ps.thr)) atomicMax(ps.thr, o);
+      if (PHASE == 1 && thr > -INFINITY) {
+        const unsigned int o = ord_f32(thr);
+        if (o > *(volatile unsigned int*)&s_thr) {
+          atomicMax(&s_thr, o);
+          if (o > __ldcg(ps.thr)) atomicMax(ps.thr, o);
+        }
       }
     }
   }
@@ -564,9 +638,35 @@ __global__ void tfim_jz_kernel(const long long* __restrict__ ptr, const int* __r
   }
 }
 
-__global__ void f64_to_f32_kernel(const double* __restrict__ a, float* __restrict__ b, int n) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    b[i] = (float)a[i];
+// f_k = g_k rounded up to float32, and the bounds the pair tiles skip by: the
+// largest f_k and |f_k| overall, per row group of DR and per column chunk of
+// CW (ordered float32, the bound array zeroed beforehand). Whole warps walk
+// 32 consecutive gains (DR and CW divide by the warp's 32).
+__global__ void gains_f32_bounds_kernel(const double* __restrict__ a, float* __restrict__ b, int n,
+                                        unsigned int* __restrict__ bound) {
+  const int lane = threadIdx.x & 31;
+  const int ng = (n - 1 + DR - 1) / DR;
+  for (long long w0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) & ~31ll; w0 < n;
+       w0 += (long long)gridDim.x * blockDim.x) {
+    const long long i = w0 + lane;
+    float f = -INFINITY;
+    if (i < n) {
+      f = __double2float_ru(a[i]);
+      b[i] = f;
+    }
+    float r = f, m = i < n ? fabsf(f) : 0.0f;
+    for (int o = 1; o < DR; o <<= 1) r = fmaxf(r, __shfl_xor_sync(0xFFFFFFFFu, r, o));
+    if ((lane & (DR - 1)) == 0 && i / DR < ng) bound[2 + i / DR] = ord_f32(r);
+    float c = r;
+    for (int o = DR; o < 32; o <<= 1) c = fmaxf(c, __shfl_xor_sync(0xFFFFFFFFu, c, o));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if (lane == 0) {
+      const unsigned int oc = ord_f32(c);
+      atomicMax(bound + 2 + ng + w0 / CW, oc);
+      atomicMax(bound, oc);
+      atomicMax(bound + 1, ord_f32(m));
+    }
+  }
 }
 
 static int grid_of(long long work, int per_block, int cap) {
@@ -631,12 +731,23 @@ pqi_status pqi_csr_single_descent(const pqi_csr* g, uint32_t* theta, double* gai
   Workspace ws(workspace, workspace_bytes);
   int* status = ws.take<int>(1);
   PQI_CHECK_ARG(status);
-  const size_t smem = (((size_t)((g->n + 31) >> 5) * 4 + 15) & ~size_t(15));
+  // segments of 256 nodes, wider when the segment keys, the rescan list and
+  // the dirty flags (13 bytes per segment) and the state bits (n / 8 bytes)
+  // would not fit in shared memory
+  const size_t bits_bytes = (((size_t)((g->n + 31) >> 5) * 4 + 15) & ~size_t(15));
+  int seg = 256;
+  auto smem_of = [&](int sg) {
+    const size_t nseg = ((size_t)g->n + sg - 1) / sg;
+    return ((nseg * 13 + 15) & ~size_t(15)) + bits_bytes;
+  };
+  while (smem_of(seg) > 200 * 1024 && seg < (1 << 20)) seg *= 2;
+  const size_t smem = smem_of(seg);
   PQI_CHECK_ARG(smem <= 200 * 1024);
   cudaStream_t s = as_stream(stream);
   PQI_TRY(cudaFuncSetAttribute(descent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  descent_kernel<<<1, 1024, smem, s>>>(g->ptr, g->col, g->val, g->n, theta, gains64, is_spin_glass,
-                                       geo, max_flips, energy_sum, flips, trace, status);
+  descent_kernel<<<1, 1024, smem, s>>>(g->ptr, g->col, g->val, g->n, seg, theta, gains64,
+                                       is_spin_glass, geo, max_flips, energy_sum, flips, trace,
+                                       status);
   PQI_LAUNCHED("csr descent_kernel");
   int hst = 0;
   PQI_TRY(cudaMemcpyAsync(&hst, status, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -644,10 +755,10 @@ pqi_status pqi_csr_single_descent(const pqi_csr* g, uint32_t* theta, double* gai
   return (pqi_status)hst;
 }
 
-pqi_status pqi_csr_double_bit_flips(const pqi_csr* g, const uint32_t* theta, const double* gains64,
-                                    int is_spin_glass, int global_size, int local_size,
-                                    float* best_energy, long long* best_index, void* workspace,
-                                    size_t workspace_bytes, void* stream) {
+static pqi_status csr_double(const pqi_csr* g, const uint32_t* theta, const double* gains64,
+                             int is_spin_glass, int global_size, int local_size, int positive,
+                             float* best_energy, long long* best_index, void* workspace,
+                             size_t workspace_bytes, void* stream) {
   PQI_CHECK_ARG(check_graph(g) && theta && best_energy && best_index && g->n >= 2);
   const int n = g->n;
   SelGeom sg;
@@ -658,11 +769,14 @@ pqi_status pqi_csr_double_bit_flips(const pqi_csr* g, const uint32_t* theta, con
   const unsigned long long pairs = (unsigned long long)n * (unsigned long long)(n - 1) / 2ull;
   geo.J = std::max<unsigned long long>(1ull, (pairs + geo.G - 1) / geo.G);
   memcpy(geo.rank, sg.rank, sizeof(geo.rank));
+  const int ng = (n - 1 + DR - 1) / DR, nc = (n + CW - 1) / CW;
+  const size_t nbound = 2 + (size_t)ng + nc;
   Workspace ws(workspace, workspace_bytes);
   unsigned long long* ctl = ws.take<unsigned long long>(2);  // prio, then vmax | thr
+  unsigned int* bound = ws.take<unsigned int>(nbound);
   float* g32 = ws.take<float>(n);
   double* gown = gains64 ? nullptr : ws.take<double>(n);
-  PQI_CHECK_ARG(ctl && g32 && (gains64 || gown));
+  PQI_CHECK_ARG(ctl && bound && g32 && (gains64 || gown));
   cudaStream_t s = as_stream(stream);
   if (!gains64) {
     pqi_status rc = pqi_csr_gains(g, theta, 1, nullptr, gown, stream);
@@ -673,10 +787,13 @@ pqi_status pqi_csr_double_bit_flips(const pqi_csr* g, const uint32_t* theta, con
   ps.prio = ctl;
   ps.vmax = reinterpret_cast<unsigned int*>(ctl + 1);
   ps.thr = ps.vmax + 1;
+  ps.bound = bound;
+  ps.positive = positive;
   PQI_TRY(cudaMemsetAsync(ctl, 0xFF, 8, s));      // prio = ~0
   PQI_TRY(cudaMemsetAsync(ctl + 1, 0, 8, s));     // vmax = thr = 0 (nothing yet)
-  f64_to_f32_kernel<<<grid_of(n, 256, 148 * 4), 256, 0, s>>>(gains64, g32, n);
-  PQI_LAUNCHED("csr f64_to_f32_kernel");
+  PQI_TRY(cudaMemsetAsync(bound, 0, nbound * sizeof(unsigned int), s));
+  gains_f32_bounds_kernel<<<grid_of(n, 256, 148 * 4), 256, 0, s>>>(gains64, g32, n, bound);
+  PQI_LAUNCHED("csr gains_f32_bounds_kernel");
   const int eg = grid_of(n, 8, 148 * 8);
   static int resident = 0;
   if (!resident) {
@@ -699,6 +816,23 @@ pqi_status pqi_csr_double_bit_flips(const pqi_csr* g, const uint32_t* theta, con
   pair_finish_kernel<<<1, 1, 0, s>>>(ps, geo, best_energy, best_index);
   PQI_LAUNCHED("csr pair_finish_kernel");
   return PQI_OK;
+}
+
+pqi_status pqi_csr_double_bit_flips(const pqi_csr* g, const uint32_t* theta, const double* gains64,
+                                    int is_spin_glass, int global_size, int local_size,
+                                    float* best_energy, long long* best_index, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
+  return csr_double(g, theta, gains64, is_spin_glass, global_size, local_size, 0, best_energy,
+                    best_index, workspace, workspace_bytes, stream);
+}
+
+pqi_status pqi_csr_improving_double_flip(const pqi_csr* g, const uint32_t* theta,
+                                         const double* gains64, int is_spin_glass,
+                                         int global_size, int local_size, float* best_energy,
+                                         long long* best_index, void* workspace,
+                                         size_t workspace_bytes, void* stream) {
+  return csr_double(g, theta, gains64, is_spin_glass, global_size, local_size, 1, best_energy,
+                    best_index, workspace, workspace_bytes, stream);
 }
 
 pqi_status pqi_csr_gray(const pqi_csr* g, const uint64_t* theta64, const double* gains64,

@@ -227,7 +227,10 @@ class DeviceGraph:
         call("pqi_single_bit_flips", ctypes.byref(self.w), _ptr(words), int(bool(is_spin_glass)), G, L, _ptr(be), _ptr(bi), wsp, wsn, self.sp())
         return be, bi
 
-    def double_bit_flips(self, words, g64, is_spin_glass, G, L):
+    def double_bit_flips(self, words, g64, is_spin_glass, G, L, improving=False):
+        """(best value, pair index) of one double-flip pass over all pairs
+        (improving: accepted for the compressed-row graph's interface; the
+        dense pass is always exact)."""
         be = torch.empty(1, dtype=torch.float32, device=self.device)
         bi = torch.empty(1, dtype=torch.int32, device=self.device)
         wsp, wsn = self.wsp(1)

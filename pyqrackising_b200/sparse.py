@@ -180,12 +180,16 @@ class SparseDeviceGraph:
                   D._ptr(be), D._ptr(bi), wsp, wsn, self.sp())
         return be, bi
 
-    def double_bit_flips(self, words, g64, is_spin_glass, G, L):
-        """(best value, 64-bit pair index) of one double-flip pass."""
+    def double_bit_flips(self, words, g64, is_spin_glass, G, L, improving=False):
+        """(best value, 64-bit pair index) of one double-flip pass. improving:
+        the same answer whenever the best value is > 0, else some value <= 0
+        (pqi_csr_improving_double_flip: at a single-flip local optimum only the
+        adjacent pairs are scored)."""
         be = torch.empty(1, dtype=torch.float32, device=self.device)
         bi = torch.empty(1, dtype=torch.int64, device=self.device)
         wsp, wsn = self.wsp()
-        _lib.call("pqi_csr_double_bit_flips", ctypes.byref(self.csr), D._ptr(words), D._ptr(g64),
+        fn = "pqi_csr_improving_double_flip" if improving else "pqi_csr_double_bit_flips"
+        _lib.call(fn, ctypes.byref(self.csr), D._ptr(words), D._ptr(g64),
                   int(bool(is_spin_glass)), G, L, D._ptr(be), D._ptr(bi), wsp, wsn, self.sp())
         return be, bi
 

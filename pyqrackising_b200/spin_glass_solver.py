@@ -110,7 +110,7 @@ def local_search(dg, theta, is_spin_glass: bool, gray_iterations: int, gray_seed
                 break
         # 2. double flips
         if n >= 2:
-            be, bi = dg.double_bit_flips(words, g64, spin, Gf, Lf)
+            be, bi = dg.double_bit_flips(words, g64, spin, Gf, Lf, improving=True)
             e = float(be.item())
             if e > 0.0:
                 k, l = pair_decode(int(bi.item()), n)

@@ -109,6 +109,49 @@ def test_csr_descent_gray_and_flips_match_dense(case, oracle_mod):
     assert torch.equal(a[2], b[2]) and torch.equal(a[3], b[3]) and torch.equal(a[4], b[4])
 
 
+@pytest.mark.parametrize("case", range(6))
+def test_csr_improving_double_flip(case, oracle_mod):
+    """pqi_csr_improving_double_flip: the exact pass's (value, index) whenever
+    that value is > 0, else a value <= 0. States: random ones (many positive
+    gains: non-adjacent pairs win), single-flip local optima (every gain <= 0:
+    only adjacent pairs can improve; integer weights leave many zero gains),
+    and local optima with one node's gain pushed up by a flip."""
+    O = oracle_mod
+    kind, W = _graphs()[case]
+    n = W.shape[0]
+    _, sg = _pair(W)
+    G, L = O.flip_geometry(n, 148)
+    rng = np.random.default_rng(40 + case)
+    seen_pos = seen_nonpos = 0
+    for trial in range(6):
+        words = sg.pack(rng.random(n) < 0.5)
+        _, g64 = sg.gains(words)
+        if trial >= 2:
+            sg.single_descent(words, g64, True, G, L, 8 * n)
+        if trial == 4:
+            sg.apply_flip(words, g64, int(rng.integers(n)))
+        if trial == 5:  # a local optimum of single and double flips
+            for _ in range(500):
+                sg.single_descent(words, g64, True, G, L, 8 * n)
+                e, i = sg.double_bit_flips(words, g64, 1, G, L)
+                if not float(e.item()) > 0.0:
+                    break
+                from pyqrackising_b200.spin_glass_solver import pair_decode
+
+                sg.apply_flip(words, g64, *pair_decode(int(i.item()), n))
+        for spin in (0, 1):
+            e0, i0 = sg.double_bit_flips(words, g64, spin, G, L)
+            e1, i1 = sg.double_bit_flips(words, g64, spin, G, L, improving=True)
+            v0, v1 = float(e0.item()), float(e1.item())
+            if v0 > 0.0:
+                seen_pos += 1
+                assert (v1, int(i1.item())) == (v0, int(i0.item()))
+            else:
+                seen_nonpos += 1
+                assert v1 <= 0.0
+    assert seen_pos and seen_nonpos
+
+
 def test_csr_solver_equals_dense_solver(monkeypatch):
     """spin_glass_solver_sparse on compressed rows (forced) and on the dense
     expansion, same graph and best_guess: the same bit string and values."""
