@@ -396,62 +396,64 @@ __global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
     float cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
     // integer estimates compare as integers (thr is then an integer value)
     int cut_i = thr > -INFINITY ? (int)thr : INT_MIN;
+    // 1. the estimates of the thread's DR x VEC pairs (unrolled, registers
+    // only): a bit per pair that reaches the cut
+    uint64_t m0 = 0ull, m1 = 0ull;
 #pragma unroll
     for (int i = 0; i < DR; ++i) {
-      const int xki = (xk >> i) & 1;
-      // (t, j) = (c mod G, c / G) of the first pair of the row that reaches
-      // the exact path (column e0), then advanced along the row's columns
-      bool have_tj = false;
-      uint32_t t0 = 0, j0 = 0;
-      int e0 = 0;
+      const uint32_t xki = (xk >> i) & 1u;
 #pragma unroll
       for (int e = 0; e < VEC; ++e) {
         // -2 W when bits k and l agree, +2 W otherwise
-        const bool agree = (((lw >> e) & 1u) == (uint32_t)xki);
-        float a = 0.0f;
-        int ai = 0;
+        const bool agree = ((lw >> e) & 1u) == xki;
         bool pass;
         if constexpr (INT) {
           const int wi = (int)w[i][e];
-          ai = fk[i] + fl[e] + (agree ? -2 * wi : 2 * wi);  // the exact value
-          pass = ai >= cut_i;
+          pass = fk[i] + fl[e] + (agree ? -2 * wi : 2 * wi) >= cut_i;
         } else {
-          a = fmaf(agree ? -2.0f : 2.0f, w[i][e], fk[i] + fl[e]);
-          pass = a >= cut;
+          pass = fmaf(agree ? -2.0f : 2.0f, w[i][e], fk[i] + fl[e]) >= cut;
         }
-        if (pass) {
-          const int k = k0 + i, l = l0 + e;
-          if (k < n - 1 && l > k && l < n) {
-            float v;
-            if constexpr (INT) {
-              v = (float)ai;  // below 2^24 in magnitude: exact
-            } else {
-              const double gk = __ldg(g64 + k), gl = __ldg(g64 + l);
-              const double wd = (double)w[i][e];
-              v = (float)(gk + gl - (agree ? 2.0 * wd : -2.0 * wd));
-            }
-            const float vu = v;
-            if (spin) v *= 2.0f;
-            if (!have_tj) {
-              const uint32_t c0 = (uint32_t)(pair_base(k, n) + (long long)(l - k - 1));
-              t0 = c0 % geo.G;
-              j0 = c0 / geo.G;
-              e0 = e;
-              have_tj = true;
-            }
-            uint32_t t = t0 + (uint32_t)(e - e0), j = j0;
-            while (t >= geo.G) {
-              t -= geo.G;
-              ++j;
-            }
-            const uint64_t kk = pair_key(v, t, j, geo);
-            best = kk > best ? kk : best;
-            if (kk != 0ull && vu > thr) {
-              thr = vu;
-              cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
-              cut_i = (int)thr;
-            }
-          }
+        const int b = i * VEC + e;
+        if (b < 64) {
+          m0 |= (uint64_t)pass << b;
+        } else {
+          m1 |= (uint64_t)pass << (b - 64);
+        }
+      }
+    }
+    // 2. the marked pairs, one code path (not unrolled): the estimate again
+    // against the cut as it rises, then the exact value and key. Its operands
+    // come back from L1 (this tile's loads).
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      uint64_t mh = h ? m1 : m0;
+      while (mh) {
+        const int b = (__ffsll((long long)mh) - 1) + 64 * h;
+        mh &= mh - 1;
+        const int i = b / VEC, e = b % VEC;
+        const int k = k0 + i, l = l0 + e;
+        if (k >= n - 1 || l <= k || l >= n) continue;
+        const WT wv = __ldg(Wp + (size_t)k * ld + l);
+        const bool agree = get_bit32(theta, (uint32_t)k) == get_bit32(theta, (uint32_t)l);
+        float v;
+        if constexpr (INT) {
+          const int ai = __ldg(gest + k) + __ldg(gest + l) + (agree ? -2 * (int)wv : 2 * (int)wv);
+          if (ai < cut_i) continue;
+          v = (float)ai;  // below 2^24 in magnitude: exact
+        } else {
+          if (fmaf(agree ? -2.0f : 2.0f, wv, __ldg(gest + k) + __ldg(gest + l)) < cut) continue;
+          const double wd = (double)wv;
+          v = (float)(__ldg(g64 + k) + __ldg(g64 + l) - (agree ? 2.0 * wd : -2.0 * wd));
+        }
+        const float vu = v;
+        if (spin) v *= 2.0f;
+        const uint32_t c = (uint32_t)(pair_base(k, n) + (long long)(l - k - 1));
+        const uint64_t kk = pair_key(v, c % geo.G, c / geo.G, geo);
+        best = kk > best ? kk : best;
+        if (kk != 0ull && vu > thr) {
+          thr = vu;
+          cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
+          cut_i = (int)thr;
         }
       }
     }
