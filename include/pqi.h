@@ -405,12 +405,19 @@ pqi_status pqi_batch_search_warp(const void* graphs, int num_graphs, const int* 
  * latency per flip than one CTA per task for large n; max_n must satisfy
  * ceil(max_n / cluster_size) <= 8192 nodes per CTA. No reference counterpart:
  * it is the single-flip descent of spin_glass_solver.py:603-717 on a cluster.
+ * reached (device int, zeroed by the caller; NULL for none): target mode.
+ * A task whose running value is >= target sets *reached = 1 (checked every
+ * 16 flips and at the task's end), and every task stops at its next 16-flip
+ * check once the flag is set, so the launch ends soon after the first task
+ * reaches the target. best_states / best_values hold each task's state and
+ * value where it stopped (status stays 0 for such a stop).
  */
 pqi_status pqi_cluster_ascent(const void* graphs, int num_graphs, const int* task_graph,
                               const uint32_t* init_states, int words_pitch, int tasks, int max_n,
                               int kind, int is_spin_glass, int cluster_size, int flip_budget,
                               uint32_t* best_states, double* best_values,
-                              unsigned long long* flips_total, int* status, void* stream);
+                              unsigned long long* flips_total, int* status, double target,
+                              int* reached, void* stream);
 
 /* ---------------------------------------------------------------------------
  * Learned flip-proposal network (no reference counterpart). bf16 storage,

@@ -118,7 +118,7 @@ SIGNATURES = {
     "pqi_batch_search_f32": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "pqi_batch_search_cta": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _vp]),
     "pqi_batch_search_warp": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _i, ctypes.c_uint64, _vp, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
-    "pqi_cluster_ascent": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, _vp]),
+    "pqi_cluster_ascent": (_i, [_vp, _i, _vp, _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _vp, _vp, _vp, ctypes.c_double, _vp, _vp]),
     "pqi_mpnn_gemm": (_i, [_i, _i, _i, _i, _i, ctypes.c_float, _vp, _i, _vp, _i, ctypes.c_float, _vp, _vp, _i, _vp, _i, _vp]),
     "pqi_mpnn_norm_adj": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
     "pqi_mpnn_features": (_i, [_vp, _vp, _vp, ctypes.c_float, _i, _vp, _vp]),

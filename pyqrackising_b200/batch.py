@@ -165,14 +165,18 @@ class BatchedSearch:
             D._ptr(best_values),
             D._ptr(flips),
             D._ptr(status),
+            ctypes.c_double(float(target) if target is not None else 0.0),
+            D._ptr(reached) if reached is not None else None,
             D.stream_ptr(self.stream),
         )
         return best_values, best_states.view(tasks, self.pitch), flips, status
 
     def cluster_ascent(self, task_graph, init_words: torch.Tensor, is_spin_glass: bool, cluster_size: int = 8,
-                       flip_budget: int | None = None):
+                       flip_budget: int | None = None, target: float | None = None):
         """Steepest ascent with one thread-block cluster per task: the same
-        result as run(rounds=0), lower latency per flip for large n."""
+        result as run(rounds=0), lower latency per flip for large n.
+        target: stop every task soon after the first one whose running value
+        reaches it (each task's state and value where it stopped)."""
         tg = torch.as_tensor(np.asarray(task_graph, dtype=np.int32)).to(self.device)
         tasks = int(tg.numel())
         best_states = torch.zeros(tasks * self.pitch, dtype=torch.int32, device=self.device)
@@ -180,6 +184,7 @@ class BatchedSearch:
         flips = torch.zeros(1, dtype=torch.int64, device=self.device)
         status = torch.zeros(1, dtype=torch.int32, device=self.device)
         budget = int(flip_budget) if flip_budget is not None else 4 * self.max_n + 64
+        reached = torch.zeros(1, dtype=torch.int32, device=self.device) if target is not None else None
         _lib.call(
             "pqi_cluster_ascent",
             D._ptr(self.desc),
@@ -197,6 +202,8 @@ class BatchedSearch:
             D._ptr(best_values),
             D._ptr(flips),
             D._ptr(status),
+            ctypes.c_double(float(target) if target is not None else 0.0),
+            D._ptr(reached) if reached is not None else None,
             D.stream_ptr(self.stream),
         )
         return best_values, best_states.view(tasks, self.pitch), flips, status

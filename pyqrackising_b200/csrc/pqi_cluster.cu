@@ -87,7 +87,8 @@ __global__ void __launch_bounds__(256) cluster_ascent_kernel(
     const ClusterGraph* __restrict__ graphs, const int* __restrict__ task_graph,
     const uint32_t* __restrict__ init_states, int words_pitch, int tasks, int spin,
     int flip_budget, uint32_t* __restrict__ best_states, double* __restrict__ best_values,
-    unsigned long long* __restrict__ flips_total, int* __restrict__ status) {
+    unsigned long long* __restrict__ flips_total, int* __restrict__ status, double target,
+    int* __restrict__ reached) {
   typedef typename std::conditional<sizeof(WT) == 1, int, double>::type GT;
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks();
@@ -100,6 +101,7 @@ __global__ void __launch_bounds__(256) cluster_ascent_kernel(
   __shared__ unsigned long long red_key[8];
   __shared__ double red_g[8];
   __shared__ int abort_flag;
+  __shared__ int stop_flag;  // written by rank 0 (target mode)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int T = blockDim.x, nwarps = T >> 5;
   if (threadIdx.x == 0) {
@@ -204,6 +206,19 @@ __global__ void __launch_bounds__(256) cluster_ascent_kernel(
           if (grp % T == (int)threadIdx.x) xm ^= 1u << (4 * (grp / T) + (rel & 3));
         }
       }
+      // target mode: a task whose value reaches the target raises the global
+      // flag; every 16 flips rank 0 reads it and hands it to the cluster's
+      // CTAs behind a cluster barrier, so all of them stop at the same flip
+      // (fields and bits then hold every accepted flip)
+      if (reached && (f & 15) == 15) {
+        if (rank == 0 && threadIdx.x == 0) {
+          if (val >= target) atomicExch(reached, 1);
+          const int r = *(volatile int*)reached;
+          for (int c = 0; c < C; ++c) *cl.map_shared_rank(&stop_flag, c) = r;
+        }
+        cl.sync();
+        if (stop_flag) break;
+      }
       // my best flip: float gain first, then the lowest node (nodes ascend)
       float bv = -INFINITY;
       int bi = -1, bx = 0;
@@ -306,6 +321,7 @@ __global__ void __launch_bounds__(256) cluster_ascent_kernel(
       val += scale * gk;
       ++nflips;
     }
+    if (reached && rank == 0 && threadIdx.x == 0 && val >= target) atomicExch(reached, 1);
     // (the last accepted flip was applied by the pass that found no further one)
     // bits back to shared memory: eight lanes assemble one 32-node word
 #pragma unroll
@@ -348,7 +364,7 @@ extern "C" pqi_status pqi_cluster_ascent(const void* graphs, int num_graphs,
                                          int is_spin_glass, int cluster_size, int flip_budget,
                                          uint32_t* best_states, double* best_values,
                                          unsigned long long* flips_total, int* status,
-                                         void* stream) {
+                                         double target, int* reached, void* stream) {
   PQI_CHECK_ARG(graphs && num_graphs > 0 && task_graph && init_states && tasks > 0 && max_n > 0);
   PQI_CHECK_ARG(best_states && best_values && flips_total && status && flip_budget > 0);
   PQI_CHECK_ARG(cluster_size == 2 || cluster_size == 4 || cluster_size == 8 ||
@@ -418,7 +434,7 @@ extern "C" pqi_status pqi_cluster_ascent(const void* graphs, int num_graphs,
     cfg.gridDim = dim3(clusters * cluster_size);
     PQI_TRY(cudaLaunchKernelEx(&cfg, kern, gd, task_graph, init_states, words_pitch, tasks,
                                is_spin_glass, flip_budget, best_states, best_values, flips_total,
-                               status));
+                               status, target, reached));
     return PQI_OK;
   };
   pqi_status st;

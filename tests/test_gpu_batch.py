@@ -141,6 +141,35 @@ def test_cluster_ascent_flip_budget_reports_timeout():
     assert torch.allclose(vals, bvals, rtol=1e-12, atol=1e-9)
 
 
+def test_cluster_ascent_target_mode(oracle_mod):
+    """Target mode: a target no task reaches leaves every result as the plain
+    run's (the 16-flip checks do not change the trajectory); a target the
+    best task reaches mid-ascent ends the launch early, with that task at or
+    above the target and each value equal to its state's exact value."""
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+    from pyqrackising_b200 import workloads as wl
+
+    O = oracle_mod
+    W = wl.sherrington_kirkpatrick(2048, seed=6)
+    bs = BatchedSearch([DeviceGraph(W)])
+    tasks = [0] * 12
+    words = bs.random_states(tasks, seed=5)
+    v0, b0, f0, s0 = bs.cluster_ascent(tasks, words, 1, cluster_size=8)
+    v1, b1, f1, s1 = bs.cluster_ascent(tasks, words, 1, cluster_size=8, target=1e300)
+    assert int(s0.item()) == int(s1.item()) == 0
+    assert torch.equal(b0, b1) and torch.equal(v0, v1) and int(f0.item()) == int(f1.item())
+    # a value every start passes well before its end: the launch stops early
+    target = 0.9 * float(v0.min())
+    v2, b2, f2, s2 = bs.cluster_ascent(tasks, words, 1, cluster_size=8, target=target)
+    assert int(s2.item()) == 0
+    assert float(v2.max()) >= target
+    assert int(f2.item()) < int(f0.item())
+    states = bs.unpack(b2, tasks)
+    for t in range(len(tasks)):
+        assert float(v2[t]) == pytest.approx(O.compute_energy(states[t], W), rel=1e-9, abs=1e-6)
+
+
 @pytest.mark.parametrize("kind", ["int", "float"])
 def test_warp_form_matches_cta_form(kind):
     """One warp per task gives the CTA form's best states, values and flip
