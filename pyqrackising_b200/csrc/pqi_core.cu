@@ -397,53 +397,48 @@ __global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
     // integer estimates compare as integers (thr is then an integer value)
     int cut_i = thr > -INFINITY ? (int)thr : INT_MIN;
     // 1. the estimates of the thread's DR x VEC pairs (unrolled, registers
-    // only): a bit per pair that reaches the cut
-    uint64_t m0 = 0ull, m1 = 0ull;
+    // only): does any reach the cut? a = f_k + f_l + 2 (-/+ W): W's sign is
+    // flipped where bits k and l agree (one three-way XOR per pair)
+    bool any = false;
 #pragma unroll
     for (int i = 0; i < DR; ++i) {
       const uint32_t xki = (xk >> i) & 1u;
 #pragma unroll
       for (int e = 0; e < VEC; ++e) {
-        // -2 W when bits k and l agree, +2 W otherwise
-        const bool agree = ((lw >> e) & 1u) == xki;
-        bool pass;
+        const uint32_t xle = (lw >> e) & 1u;
         if constexpr (INT) {
+          const int m = -(int)(xki ^ xle);  // 0 where the bits agree, else -1
           const int wi = (int)w[i][e];
-          pass = fk[i] + fl[e] + (agree ? -2 * wi : 2 * wi) >= cut_i;
+          any |= fk[i] + fl[e] - 2 * ((wi ^ m) - m) >= cut_i;
         } else {
-          pass = fmaf(agree ? -2.0f : 2.0f, w[i][e], fk[i] + fl[e]) >= cut;
-        }
-        const int b = i * VEC + e;
-        if (b < 64) {
-          m0 |= (uint64_t)pass << b;
-        } else {
-          m1 |= (uint64_t)pass << (b - 64);
+          const float cw =
+              __uint_as_float(__float_as_uint(w[i][e]) ^ ((xki ^ xle ^ 1u) << 31));
+          any |= fmaf(2.0f, cw, fk[i] + fl[e]) >= cut;
         }
       }
     }
-    // 2. the marked pairs, one code path (not unrolled): the estimate again
-    // against the cut as it rises, then the exact value and key. Its operands
-    // come back from L1 (this tile's loads).
+    // 2. a tile with a pair at the cut (rare once the threshold has risen):
+    // every pair again in one code path (not unrolled), its estimate against
+    // the cut as it rises, then the exact value and key. The operands come
+    // back from L1 (this tile's loads).
+    if (any) {
 #pragma unroll 1
-    for (int h = 0; h < 2; ++h) {
-      uint64_t mh = h ? m1 : m0;
-      while (mh) {
-        const int b = (__ffsll((long long)mh) - 1) + 64 * h;
-        mh &= mh - 1;
+      for (int b = 0; b < DR * VEC; ++b) {
         const int i = b / VEC, e = b % VEC;
         const int k = k0 + i, l = l0 + e;
         if (k >= n - 1 || l <= k || l >= n) continue;
         const WT wv = __ldg(Wp + (size_t)k * ld + l);
-        const bool agree = get_bit32(theta, (uint32_t)k) == get_bit32(theta, (uint32_t)l);
+        const uint32_t flip = (uint32_t)(get_bit32(theta, (uint32_t)k) ^ get_bit32(theta, (uint32_t)l)) ^ 1u;
         float v;
         if constexpr (INT) {
-          const int ai = __ldg(gest + k) + __ldg(gest + l) + (agree ? -2 * (int)wv : 2 * (int)wv);
+          const int ai = __ldg(gest + k) + __ldg(gest + l) + (flip ? -2 * (int)wv : 2 * (int)wv);
           if (ai < cut_i) continue;
           v = (float)ai;  // below 2^24 in magnitude: exact
         } else {
-          if (fmaf(agree ? -2.0f : 2.0f, wv, __ldg(gest + k) + __ldg(gest + l)) < cut) continue;
+          const float cw = __uint_as_float(__float_as_uint(wv) ^ (flip << 31));
+          if (fmaf(2.0f, cw, __ldg(gest + k) + __ldg(gest + l)) < cut) continue;
           const double wd = (double)wv;
-          v = (float)(__ldg(g64 + k) + __ldg(g64 + l) - (agree ? 2.0 * wd : -2.0 * wd));
+          v = (float)(__ldg(g64 + k) + __ldg(g64 + l) - (flip ? 2.0 * wd : -2.0 * wd));
         }
         const float vu = v;
         if (spin) v *= 2.0f;
