@@ -165,8 +165,6 @@ class BatchedSearch:
             D._ptr(best_values),
             D._ptr(flips),
             D._ptr(status),
-            ctypes.c_double(float(target) if target is not None else 0.0),
-            D._ptr(reached) if reached is not None else None,
             D.stream_ptr(self.stream),
         )
         return best_values, best_states.view(tasks, self.pitch), flips, status

@@ -8,6 +8,7 @@
 #include <type_traits>
 
 #include "pqi_common.cuh"
+#include "pqi_tc.cuh"
 
 namespace pqi {
 
@@ -468,6 +469,207 @@ __global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
 // ---------------------------------------------------------------------------
 // Apply one or two flips to (theta, gains64). x = 2s - 1 of the state before.
 
+// The same pass with W streamed through shared memory: one persistent CTA per
+// SM, a producer warp copying each tile's DR row segments of 4 KB
+// (cp.async.bulk, completion counted on the stage's mbarrier) into a ring of
+// DS_STAGES stages, and DS_CONSUMERS threads that score the tile from shared
+// memory (the estimate pass, then the exact path for flagged tiles, as in
+// double_tile_kernel) and release the stage. The copies run up to
+// DS_STAGES tiles ahead of the scoring, so HBM sees a deep queue of large
+// requests whatever the scoring's latency.
+constexpr int DS_STAGES = 6;
+constexpr int DS_CONSUMERS = 256;
+constexpr int DS_THREADS = DS_CONSUMERS + 32;
+constexpr int DS_ROW_BYTES = 4096;
+constexpr int DS_TILE_BYTES = DR * DS_ROW_BYTES;
+constexpr int DS_SMEM = DS_STAGES * DS_TILE_BYTES;
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          tc::smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+      : "memory");
+}
+
+template <typename WT>
+__global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
+    const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
+    const double* __restrict__ g64, const void* __restrict__ gest_v, int spin, SelGeom geo,
+    unsigned long long* key, unsigned int* gthr) {
+  constexpr int VEC = 16 / (int)sizeof(WT);  // columns per consumer thread
+  constexpr int CW = VEC * DS_CONSUMERS;    // columns per tile (4 KB of a row)
+  constexpr bool INT = sizeof(WT) == 1;
+  typedef typename std::conditional<INT, int, float>::type ET;
+  const ET* __restrict__ gest = static_cast<const ET*>(gest_v);
+  extern __shared__ __align__(1024) unsigned char ring[];
+  __shared__ __align__(8) uint64_t full_bar[DS_STAGES];
+  __shared__ __align__(8) uint64_t empty_bar[DS_STAGES];
+  __shared__ uint64_t scratch[32];
+  __shared__ unsigned int s_thr;
+  __shared__ int s_fail;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < DS_STAGES; ++st) {
+      tc::mbar_init(&full_bar[st], 1);
+      tc::mbar_init(&empty_bar[st], DS_CONSUMERS / 32);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    s_thr = 0u;
+    s_fail = 0;
+  }
+  __syncthreads();
+  const int ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
+  const int nc = (n + CW - 1) / CW;      // column chunks
+  const long long total = (long long)ng * nc;
+  uint64_t best = 0;
+  if (warp == DS_CONSUMERS / 32) {
+    // producer: the tiles of this CTA in order, each into the next stage once
+    // the consumers have released that stage's previous tile
+    if (lane == 0) {
+      int it = 0;
+      for (long long tau = blockIdx.x; tau < total; tau += gridDim.x) {
+        const int rg = (int)(tau / nc), c = (int)(tau - (long long)(tau / nc) * nc);
+        if ((c + 1) * CW <= rg * DR + 1) continue;  // wholly at or below the diagonal
+        const int st = it % DS_STAGES;
+        const uint32_t use = (uint32_t)(it / DS_STAGES);
+        if (use > 0 && !tc::mbar_wait(&empty_bar[st], (use - 1) & 1u)) {
+          s_fail = 1;
+          break;
+        }
+        // the row segments: up to CW columns, within the padded row (ld is a
+        // multiple of 128, so the size is a multiple of 512 bytes)
+        const int col0 = c * CW;
+        const uint32_t bytes = (uint32_t)(min(CW, ld - col0) * (int)sizeof(WT));
+        tc::mbar_expect_tx(&full_bar[st], bytes * DR);
+        unsigned char* dst = ring + (size_t)st * DS_TILE_BYTES;
+#pragma unroll
+        for (int i = 0; i < DR; ++i) {
+          const int k = min(rg * DR + i, n - 1);
+          bulk_copy_g2s(dst + i * DS_ROW_BYTES, Wp + (size_t)k * ld + col0, bytes, &full_bar[st]);
+        }
+        ++it;
+      }
+    }
+  } else {
+    float thr = -INFINITY;
+    int it = 0;
+    for (long long tau = blockIdx.x; tau < total; tau += gridDim.x) {
+      const int rg = (int)(tau / nc), c = (int)(tau - (long long)(tau / nc) * nc);
+      if ((c + 1) * CW <= rg * DR + 1) continue;
+      const int st = it % DS_STAGES;
+      const uint32_t use = (uint32_t)(it / DS_STAGES);
+      ++it;
+      const int k0 = rg * DR;
+      const int l0 = c * CW + (int)threadIdx.x * VEC;
+      // the tile's rows: gains and bits (the same for every thread), this
+      // thread's columns: loaded while the stage's copies land
+      ET fk[DR];
+      uint32_t xk = 0;
+      float gt = 0.0f;
+#pragma unroll
+      for (int i = 0; i < DR; ++i) {
+        const int k = min(k0 + i, n - 1);
+        fk[i] = __ldg(gest + k);
+        if constexpr (!INT) gt = fmaxf(gt, fabsf(fk[i]));
+        xk |= (uint32_t)get_bit32(theta, k) << i;
+      }
+      ET fl[VEC];
+      float flmax = 0.0f;
+      const uint32_t lw = l0 < n ? __ldg(theta + (l0 >> 5)) >> (l0 & 31) : 0u;
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) {
+        const int l = l0 + e;
+        fl[e] = l < n ? __ldg(gest + l) : ET(0);
+        if constexpr (!INT) flmax = fmaxf(flmax, fabsf(fl[e]));
+      }
+      thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(gthr))));
+      if (!tc::mbar_wait_warp(&full_bar[st], use & 1u)) {
+        s_fail = 1;
+        break;
+      }
+      const unsigned char* tile = ring + (size_t)st * DS_TILE_BYTES + threadIdx.x * 16;
+      WT w[DR][VEC];
+#pragma unroll
+      for (int i = 0; i < DR; ++i) {
+        const int4 v = *reinterpret_cast<const int4*>(tile + i * DS_ROW_BYTES);
+        memcpy(&w[i][0], &v, 16);
+      }
+      const float base = gt + flmax;
+      float cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
+      int cut_i = thr > -INFINITY ? (int)thr : INT_MIN;
+      // (columns past the copied row segment hold stale bytes: such a thread
+      // has no column below n and skips the estimates)
+      bool any = false;
+#pragma unroll
+      for (int i = 0; i < DR; ++i) {
+        const uint32_t xki = (xk >> i) & 1u;
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) {
+          const uint32_t xle = (lw >> e) & 1u;
+          if constexpr (INT) {
+            const int m = -(int)(xki ^ xle);
+            const int wi = (int)w[i][e];
+            any |= fk[i] + fl[e] - 2 * ((wi ^ m) - m) >= cut_i;
+          } else {
+            const float cw =
+                __uint_as_float(__float_as_uint(w[i][e]) ^ ((xki ^ xle ^ 1u) << 31));
+            any |= fmaf(2.0f, cw, fk[i] + fl[e]) >= cut;
+          }
+        }
+      }
+      if (any && l0 < n) {
+        const WT* tw = reinterpret_cast<const WT*>(ring + (size_t)st * DS_TILE_BYTES);
+#pragma unroll 1
+        for (int b = 0; b < DR * VEC; ++b) {
+          const int i = b / VEC, e = b % VEC;
+          const int k = k0 + i, l = l0 + e;
+          if (k >= n - 1 || l <= k || l >= n) continue;
+          const WT wv = tw[i * (DS_ROW_BYTES / (int)sizeof(WT)) + (l - c * CW)];
+          const uint32_t flip =
+              (uint32_t)(get_bit32(theta, (uint32_t)k) ^ get_bit32(theta, (uint32_t)l)) ^ 1u;
+          float v;
+          if constexpr (INT) {
+            const int ai = __ldg(gest + k) + __ldg(gest + l) + (flip ? -2 * (int)wv : 2 * (int)wv);
+            if (ai < cut_i) continue;
+            v = (float)ai;
+          } else {
+            const float cw = __uint_as_float(__float_as_uint(wv) ^ (flip << 31));
+            if (fmaf(2.0f, cw, __ldg(gest + k) + __ldg(gest + l)) < cut) continue;
+            const double wd = (double)wv;
+            v = (float)(__ldg(g64 + k) + __ldg(g64 + l) - (flip ? 2.0 * wd : -2.0 * wd));
+          }
+          const float vu = v;
+          if (spin) v *= 2.0f;
+          const uint32_t cidx = (uint32_t)(pair_base(k, n) + (long long)(l - k - 1));
+          const uint64_t kk = pair_key(v, cidx % geo.G, cidx / geo.G, geo);
+          best = kk > best ? kk : best;
+          if (kk != 0ull && vu > thr) {
+            thr = vu;
+            cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
+            cut_i = (int)thr;
+          }
+        }
+      }
+      // the stage back to the producer (this warp's reads are done)
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&empty_bar[st]);
+      if (thr > -INFINITY) {
+        const unsigned int o = ord_f32(thr);
+        if (o > *(volatile unsigned int*)&s_thr) {
+          atomicMax(&s_thr, o);
+          if (o > __ldcg(gthr)) atomicMax(gthr, o);
+        }
+      }
+    }
+  }
+  best = block_max_u64(best, scratch);
+  // a wait that ran out leaves no result (key 0: value -inf, index -1)
+  if (threadIdx.x == 0 && best && !s_fail) atomicMax(key, (unsigned long long)best);
+}
+
 template <typename WT>
 __global__ void apply_flip_gains_kernel(const WT* __restrict__ Wp, int ld, int n,
                                         const uint32_t* __restrict__ theta,
@@ -819,25 +1021,28 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     gains_to_estimate_kernel<float><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(gains64, n, static_cast<float*>(gest));
   }
   PQI_LAUNCHED("gains_to_estimate_kernel");
-  // one resident wave of blocks, persistent over the tiles
-  static int resident[2] = {0, 0};
+  // one persistent CTA per SM (the stage ring takes most of shared memory)
+  static int sms = 0;
+  static bool attr_set[2] = {false, false};
   const int i8 = w->kind == PQI_W_I8 ? 1 : 0;
-  if (!resident[i8]) {
-    int dev = 0, sms = 0, per_sm = 0;
+  if (!sms) {
+    int dev = 0;
     PQI_TRY(cudaGetDevice(&dev));
     PQI_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const void* fn = i8 ? (const void*)double_tile_kernel<int8_t> : (const void*)double_tile_kernel<float>;
-    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, DTHREADS, 0));
-    resident[i8] = std::max(1, sms * std::max(1, per_sm));
+  }
+  if (!attr_set[i8]) {
+    const void* fn = i8 ? (const void*)double_stream_kernel<int8_t> : (const void*)double_stream_kernel<float>;
+    PQI_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, DS_SMEM));
+    attr_set[i8] = true;
   }
   if (i8) {
-    double_tile_kernel<int8_t><<<resident[i8], DTHREADS, 0, s>>>(w->W_i8, w->ld, n, theta, gains64, gest,
-                                                                is_spin_glass, geo, key, gthr);
+    double_stream_kernel<int8_t><<<sms, DS_THREADS, DS_SMEM, s>>>(w->W_i8, w->ld, n, theta, gains64, gest,
+                                                                  is_spin_glass, geo, key, gthr);
   } else {
-    double_tile_kernel<float><<<resident[i8], DTHREADS, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64, gest,
-                                                               is_spin_glass, geo, key, gthr);
+    double_stream_kernel<float><<<sms, DS_THREADS, DS_SMEM, s>>>(w->W_f32z, w->ld, n, theta, gains64, gest,
+                                                                 is_spin_glass, geo, key, gthr);
   }
-  PQI_LAUNCHED("double_tile_kernel");
+  PQI_LAUNCHED("double_stream_kernel");
   select_finish_kernel<<<1, 1, 0, s>>>(key, geo, best_energy, best_index);
   PQI_LAUNCHED("select_finish_kernel");
   return PQI_OK;
