@@ -12,6 +12,10 @@ Public API (same signatures and return tuples as the reference):
                    repulsion_base, is_maxcut_gpu, verbose, time_limit,
                    gray_iterations, gray_seed_multiple[, batch_size])
   solve_maxcut_bnb_sparse (same, CSR or graph input)
+  tsp_symmetric / tsp_asymmetric(G, start_node, end_node, quality, shots,
+                  anneal_t, anneal_h, repulsion_base, monte_carlo, k_neighbors,
+                  is_cyclic, multi_start, is_top_level, is_parallel, parallel_level)
+                  (MAXCUT splits on the device for monte_carlo=False)
 
 All arithmetic on the coupling matrix runs in libpqi.so (hand-written sm_100a
 CUDA behind the C ABI in include/pqi.h); there is no CPU fallback.
@@ -24,4 +28,13 @@ from .sparse import maxcut_tfim_sparse, spin_glass_solver_hybrid, spin_glass_sol
 
 __all__ = ["maxcut_tfim", "spin_glass_solver", "maxcut_tfim_sparse", "spin_glass_solver_sparse",
            "spin_glass_solver_hybrid",
-           "solve_maxcut_bnb", "solve_maxcut_bnb_sparse"]
+           "solve_maxcut_bnb", "solve_maxcut_bnb_sparse", "tsp_symmetric", "tsp_asymmetric"]
+
+
+def __getattr__(name):
+    # the TSP module (numba-compiled path heuristics) loads on first use
+    if name in ("tsp_symmetric", "tsp_asymmetric"):
+        from . import tsp
+
+        return getattr(tsp, name)
+    raise AttributeError(name)
