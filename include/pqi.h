@@ -380,6 +380,14 @@ pqi_status pqi_batch_search_cta(const void* graphs, int num_graphs, const int* t
  * every row group in registers. Results are identical. */
 pqi_status pqi_batch_set_staging(int on);
 
+/* Cross-check knob (no reference counterpart): on (default) the batched
+ * searches and the cluster ascent of graphs of 64 nodes or more compute the
+ * starting local fields of all dense-graph tasks first, one pass over W per
+ * tile of 64 tasks x 64 nodes (float64 sums, u ascending: the search
+ * kernels' own order), into a buffer from the device's stream-ordered memory
+ * pool; off, every task sums its own fields from W. */
+pqi_status pqi_batch_set_start_pass(int on);
+
 /*
  * pqi_batch_search with one warp per task instead of one CTA: the same search,
  * selection rule, kick stream, outputs and status, for graphs with

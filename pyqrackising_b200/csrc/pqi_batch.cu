@@ -303,6 +303,97 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   }
 }
 
+// Starting local fields of many tasks at once, for graphs without row lists:
+// Y[t][v] = sum_u x_tu W[u][v] (x = +-1), u ascending from 0 - the order and
+// the accumulation type (float64 for float weights, int32 for int8) of the
+// search kernel's own column-order sum, so the fields are the same numbers.
+// A CTA takes SF_T tasks x SF_V nodes: each row chunk of W (SF_U rows) is
+// read once into shared memory (converted once) and used by all SF_T tasks,
+// instead of every task streaming all of W. The tasks of a tile may belong to
+// different graphs: the tile runs once per distinct graph among its tasks
+// (one pass for tasks grouped by graph). Row-list graphs are skipped (the
+// search kernel sums their nonzeros itself).
+constexpr int SF_T = 64;
+constexpr int SF_V = 64;
+constexpr int SF_U = 32;
+
+template <typename WT>
+__global__ void __launch_bounds__(256) start_fields_kernel(
+    const BatchGraph* __restrict__ graphs, const int* __restrict__ task_graph,
+    const uint32_t* __restrict__ init_states, int words_pitch, int tasks,
+    double* __restrict__ Y, int ypitch) {
+  typedef typename std::conditional<sizeof(WT) == 1, int, double>::type AT;
+  __shared__ __align__(16) AT Ws[SF_U][SF_V];
+  __shared__ uint32_t Xs[SF_T];
+  __shared__ int gid[SF_T];
+  const int t0 = blockIdx.x * SF_T, v0 = blockIdx.y * SF_V;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // nodes v0+4tx+i, tasks t0+4ty+j
+  if (threadIdx.x < SF_T) gid[threadIdx.x] = t0 + (int)threadIdx.x < tasks ? task_graph[t0 + threadIdx.x] : -1;
+  __syncthreads();
+  uint64_t done = 0;  // tile tasks handled (the same in every thread)
+  for (int i = 0; i < SF_T; ++i)
+    if (gid[i] < 0) done |= 1ull << i;
+  while (done != ~0ull) {
+    const int g = gid[__ffsll((long long)~done) - 1];
+    uint64_t mine = 0;
+    for (int i = 0; i < SF_T; ++i)
+      if (gid[i] == g) mine |= 1ull << i;
+    done |= mine;
+    const BatchGraph G = graphs[g];
+    if (G.adj_ptr || v0 >= G.n) continue;
+    const WT* __restrict__ W = static_cast<const WT*>(G.W);
+    const int n = G.n;
+    AT acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+    for (int u0 = 0; u0 < n; u0 += SF_U) {
+      __syncthreads();  // the previous chunk's reads are done
+      for (int idx = threadIdx.x; idx < SF_U * SF_V; idx += blockDim.x) {
+        const int r = idx / SF_V, c = idx - r * SF_V;
+        const int u = u0 + r, v = v0 + c;
+        Ws[r][c] = (u < n && v < n) ? (AT)__ldg(W + (size_t)u * G.ld + v) : (AT)0;
+      }
+      if (threadIdx.x < SF_T)
+        Xs[threadIdx.x] = ((mine >> threadIdx.x) & 1ull)
+                              ? __ldg(init_states + (size_t)(t0 + threadIdx.x) * words_pitch + (u0 >> 5))
+                              : 0u;
+      __syncthreads();
+      uint32_t xw[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) xw[j] = Xs[4 * ty + j];
+      auto row = [&](int r) {
+        AT w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) w[i] = Ws[r][4 * tx + i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const bool bit = (xw[j] >> r) & 1u;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) acc[i][j] += bit ? w[i] : -w[i];
+        }
+      };
+      if (n - u0 >= SF_U) {
+#pragma unroll 8
+        for (int r = 0; r < SF_U; ++r) row(r);
+      } else {
+        for (int r = 0; r < n - u0; ++r) row(r);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (!((mine >> (4 * ty + j)) & 1ull)) continue;
+      const int t = t0 + 4 * ty + j;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int v = v0 + 4 * tx + i;
+        if (v < n) Y[(size_t)t * ypitch + v] = (double)acc[i][j];
+      }
+    }
+  }
+}
+
 // F32: float graphs keep float32 local fields (half the shared memory and
 // fewer registers, so more resident tasks per SM); gains, the selection rule
 // and the float64 running value are unchanged in form.
@@ -318,7 +409,7 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
     int kick, int flip_budget, uint64_t seed, const double* __restrict__ kick_cdf,
     const long long* __restrict__ cdf_offset, uint32_t* __restrict__ best_states,
     double* __restrict__ best_values, unsigned long long* __restrict__ flips_total,
-    int* __restrict__ status) {
+    int* __restrict__ status, const double* __restrict__ start_fields, int fields_pitch) {
   typedef typename std::conditional<
       sizeof(WT) == 1, int, typename std::conditional<F32, float, double>::type>::type GT;
   extern __shared__ __align__(16) unsigned char smem[];
@@ -362,7 +453,11 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
       c.g[fpos<BT>(v)] = (GT)acc;
       qpart += ((c.bits[v >> 5] >> (v & 31)) & 1) ? (double)acc : -(double)acc;
     };
-    if (G.adj_ptr) {
+    if (start_fields && !G.adj_ptr) {
+      // computed for all tasks beforehand (start_fields_kernel)
+      const double* __restrict__ yrow = start_fields + (size_t)task * fields_pitch;
+      for (int v = threadIdx.x; v < n; v += blockDim.x) store_field(v, (AT)yrow[v]);
+    } else if (G.adj_ptr) {
       for (int v = threadIdx.x; v < n; v += blockDim.x) {
         AT acc = 0;
         const long long e1 = G.adj_ptr[v + 1];
@@ -737,6 +832,11 @@ __global__ void __launch_bounds__(128) warp_search_kernel(
   if (lane == 0 && nflips_all) atomicAdd(flips_total, nflips_all);
 }
 
+// Starting fields of the dense-graph tasks into a stream-ordered buffer (below).
+pqi_status start_fields(const void* graphs, const int* task_graph, const uint32_t* init_states,
+                        int words_pitch, int tasks, int max_n, bool i8, cudaStream_t s,
+                        double** out, int* pitch);
+
 }  // namespace pqi
 
 using namespace pqi;
@@ -748,6 +848,45 @@ size_t pqi_batch_graph_desc_bytes(void) { return sizeof(BatchGraph); }
 }  // extern "C"
 
 static int g_batch_no_stage = 0;
+static int g_batch_no_start_pass = 0;
+
+// Starting fields of the dense-graph tasks (start_fields_kernel) into a
+// buffer from the stream-ordered pool, freed by the caller after its launch
+// (cudaFreeAsync on the same stream). *out stays null (the search kernels
+// then sum their own fields) below 64 nodes or when switched off.
+pqi_status pqi::start_fields(const void* graphs, const int* task_graph,
+                             const uint32_t* init_states, int words_pitch, int tasks, int max_n,
+                             bool i8, cudaStream_t s, double** out, int* pitch) {
+  const BatchGraph* gd = static_cast<const BatchGraph*>(graphs);
+  *out = nullptr;
+  *pitch = 0;
+  if (max_n < 64 || g_batch_no_start_pass) return PQI_OK;
+  static bool pool_kept = false;
+  if (!pool_kept) {
+    // keep freed pool memory for the next launch instead of returning it at
+    // every synchronisation
+    int dev = 0;
+    cudaMemPool_t pool;
+    PQI_TRY(cudaGetDevice(&dev));
+    PQI_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t keep = UINT64_MAX;
+    PQI_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    pool_kept = true;
+  }
+  const int yp = (max_n + 3) & ~3;
+  double* y = nullptr;
+  PQI_TRY(cudaMallocAsync(reinterpret_cast<void**>(&y), (size_t)tasks * yp * sizeof(double), s));
+  const dim3 grid((unsigned)((tasks + SF_T - 1) / SF_T), (unsigned)((max_n + SF_V - 1) / SF_V));
+  if (i8) {
+    start_fields_kernel<int8_t><<<grid, 256, 0, s>>>(gd, task_graph, init_states, words_pitch, tasks, y, yp);
+  } else {
+    start_fields_kernel<float><<<grid, 256, 0, s>>>(gd, task_graph, init_states, words_pitch, tasks, y, yp);
+  }
+  PQI_LAUNCHED("start_fields_kernel");
+  *out = y;
+  *pitch = yp;
+  return PQI_OK;
+}
 
 static pqi_status batch_search_impl(const void* graphs, int num_graphs, const int* task_graph,
                                     const uint32_t* init_states, int words_pitch, int tasks,
@@ -785,6 +924,12 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   // persistent grid: exactly the CTAs that are resident at once
   int per_sm = 1;
   const BatchGraph* gd = static_cast<const BatchGraph*>(graphs);
+  // the starting fields of dense-graph tasks as one pass over W per task tile
+  double* sf = nullptr;
+  int sf_pitch = 0;
+  pqi_status sfst = start_fields(gd, task_graph, init_states, words_pitch, tasks, max_n, i8, s, &sf,
+                                 &sf_pitch);
+  if (sfst != PQI_OK) return sfst;
   // row loads per thread: groups of four nodes, CH groups in flight per chunk
   // (the whole row for n <= 4 * 256 * CH). CH = 4 keeps three CTAs per SM
   // within the register file (8 groups spill at that occupancy and run slower
@@ -801,7 +946,7 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
     batch_search_kernel<WT_, CH_, F_, S_, BT_><<<grid, BT_, smem_all, s>>>(                    \
         gd, task_graph, init_states, words_pitch, tasks, is_spin_glass, rounds, kick,          \
         flip_budget, seed, kick_cdf, cdf_offset, best_states, best_values, flips_total,        \
-        status);                                                                               \
+        status, sf, sf_pitch);                                                                 \
   } while (0)
   if (bt == 64) {  // smallest graphs: four groups per thread cover n <= 1024
     if (i8) {
@@ -866,10 +1011,16 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   }
 #undef PQI_BATCH_LAUNCH
   PQI_LAUNCHED("batch_search_kernel");
+  if (sf) PQI_TRY(cudaFreeAsync(sf, s));
   return PQI_OK;
 }
 
 extern "C" {
+
+pqi_status pqi_batch_set_start_pass(int on) {
+  g_batch_no_start_pass = on ? 0 : 1;
+  return PQI_OK;
+}
 
 pqi_status pqi_batch_set_staging(int on) {
   g_batch_no_stage = on ? 0 : 1;

@@ -36,6 +36,11 @@ namespace cg = cooperative_groups;
 
 namespace pqi {
 
+// Starting fields of the dense-graph tasks (pqi_batch.cu), freed by the caller.
+pqi_status start_fields(const void* graphs, const int* task_graph, const uint32_t* init_states,
+                        int words_pitch, int tasks, int max_n, bool i8, cudaStream_t s,
+                        double** out, int* pitch);
+
 struct ClusterGraph {  // same layout as the batched search's graph descriptor
   const void* W;
   int n;
@@ -88,7 +93,7 @@ __global__ void __launch_bounds__(256) cluster_ascent_kernel(
     const uint32_t* __restrict__ init_states, int words_pitch, int tasks, int spin,
     int flip_budget, uint32_t* __restrict__ best_states, double* __restrict__ best_values,
     unsigned long long* __restrict__ flips_total, int* __restrict__ status, double target,
-    int* __restrict__ reached) {
+    int* __restrict__ reached, const double* __restrict__ start_fields, int fields_pitch) {
   typedef typename std::conditional<sizeof(WT) == 1, int, double>::type GT;
   cg::cluster_group cl = cg::this_cluster();
   const int C = (int)cl.num_blocks();
@@ -124,16 +129,22 @@ __global__ void __launch_bounds__(256) cluster_ascent_kernel(
     GT* y0 = reinterpret_cast<GT*>(smem + (((size_t)n32 * 4 + 15) & ~size_t(15)));
     for (int w = threadIdx.x; w < n32; w += T) bits[w] = init_states[(size_t)task * words_pitch + w];
     __syncthreads();
-    // starting local fields of the slice, one warp per row
-    for (int v = lo + warp; v < hi; v += nwarps) {
-      const WT* row = W + (size_t)v * G.ld;
-      GT acc = 0;
-      for (int u = lane; u < n; u += 32) {
-        const GT w = (GT)row[u];
-        acc += ((bits[u >> 5] >> (u & 31)) & 1) ? w : -w;
+    // starting local fields of the slice: computed beforehand for all tasks
+    // (start_fields_kernel), else one warp per row
+    if (start_fields && !G.adj_ptr) {
+      const double* __restrict__ yrow = start_fields + (size_t)task * fields_pitch;
+      for (int v = lo + (int)threadIdx.x; v < hi; v += T) y0[v - lo] = (GT)yrow[v];
+    } else {
+      for (int v = lo + warp; v < hi; v += nwarps) {
+        const WT* row = W + (size_t)v * G.ld;
+        GT acc = 0;
+        for (int u = lane; u < n; u += 32) {
+          const GT w = (GT)row[u];
+          acc += ((bits[u >> 5] >> (u & 31)) & 1) ? w : -w;
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+        if (lane == 0) y0[v - lo] = acc;
       }
-      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
-      if (lane == 0) y0[v - lo] = acc;
     }
     __syncthreads();
     GT y[4 * NG];
@@ -401,6 +412,14 @@ extern "C" pqi_status pqi_cluster_ascent(const void* graphs, int num_graphs,
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   const ClusterGraph* gd = static_cast<const ClusterGraph*>(graphs);
+  // the starting fields of dense-graph tasks, one pass over W per task tile
+  double* sf = nullptr;
+  int sf_pitch = 0;
+  {
+    pqi_status r = start_fields(graphs, task_graph, init_states, words_pitch, tasks, max_n, i8,
+                                as_stream(stream), &sf, &sf_pitch);
+    if (r != PQI_OK) return r;
+  }
   auto launch = [&](auto kern) -> pqi_status {
     PQI_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (cluster_size > 8)
@@ -434,7 +453,7 @@ extern "C" pqi_status pqi_cluster_ascent(const void* graphs, int num_graphs,
     cfg.gridDim = dim3(clusters * cluster_size);
     PQI_TRY(cudaLaunchKernelEx(&cfg, kern, gd, task_graph, init_states, words_pitch, tasks,
                                is_spin_glass, flip_budget, best_states, best_values, flips_total,
-                               status, target, reached));
+                               status, target, reached, (const double*)sf, sf_pitch));
     return PQI_OK;
   };
   pqi_status st;
@@ -451,5 +470,6 @@ extern "C" pqi_status pqi_cluster_ascent(const void* graphs, int num_graphs,
   }
   if (st != PQI_OK) return st;
   PQI_LAUNCHED("cluster_ascent_kernel");
+  if (sf) PQI_TRY(cudaFreeAsync(sf, as_stream(stream)));
   return PQI_OK;
 }

@@ -601,22 +601,39 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
       // (columns past the copied row segment hold stale bytes: such a thread
       // has no column below n and skips the estimates)
       bool any = false;
+      if constexpr (INT) {
 #pragma unroll
-      for (int i = 0; i < DR; ++i) {
-        const uint32_t xki = (xk >> i) & 1u;
+        for (int i = 0; i < DR; ++i) {
+          const uint32_t xki = (xk >> i) & 1u;
 #pragma unroll
-        for (int e = 0; e < VEC; ++e) {
-          const uint32_t xle = (lw >> e) & 1u;
-          if constexpr (INT) {
-            const int m = -(int)(xki ^ xle);
+          for (int e = 0; e < VEC; ++e) {
+            const int m = -(int)(xki ^ ((lw >> e) & 1u));
             const int wi = (int)w[i][e];
             any |= fk[i] + fl[e] - 2 * ((wi ^ m) - m) >= cut_i;
-          } else {
-            const float cw =
-                __uint_as_float(__float_as_uint(w[i][e]) ^ ((xki ^ xle ^ 1u) << 31));
-            any |= fmaf(2.0f, cw, fk[i] + fl[e]) >= cut;
           }
         }
+      } else {
+        // the largest estimate of the thread's pairs, f_k + (f_l + 2 (-/+ W)):
+        // W's sign bit flipped by a row mask and a column mask (one three-way
+        // XOR), one FMA and one max per pair. (The grouping differs from the
+        // exact path's (f_k + f_l) + 2 (-/+ W) by a few units in the last
+        // place, far inside the cut's 2^-20 margin.)
+        uint32_t cm[VEC];
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) cm[e] = ((lw >> e) & 1u) << 31;
+        float amax = -INFINITY;
+#pragma unroll
+        for (int i = 0; i < DR; ++i) {
+          const uint32_t rm = (((xk >> i) & 1u) ^ 1u) << 31;
+          float r = -INFINITY;
+#pragma unroll
+          for (int e = 0; e < VEC; ++e) {
+            const float cw = __uint_as_float(__float_as_uint(w[i][e]) ^ rm ^ cm[e]);
+            r = fmaxf(r, fmaf(2.0f, cw, fl[e]));
+          }
+          amax = fmaxf(amax, fk[i] + r);
+        }
+        any = amax >= cut;
       }
       if (any && l0 < n) {
         const WT* tw = reinterpret_cast<const WT*>(ring + (size_t)st * DS_TILE_BYTES);

@@ -365,3 +365,44 @@ def test_row_list_starts_match_dense_starts():
                     x = np.where(bits, 1.0, -1.0)
                     assert float(a[0][t]) == pytest.approx(-0.5 * x @ W @ x, rel=1e-9, abs=1e-9)
                     assert np.all(x * (W @ x) <= 1e-9 * np.abs(W).sum(axis=1).max())
+
+
+@pytest.mark.parametrize("kind", ["int", "float"])
+def test_start_pass_gives_the_per_task_fields(kind, oracle_mod):
+    """The batched starting-field pass (one pass over W per tile of 64 tasks x
+    64 nodes) against every task summing its own fields: dense graphs (no row
+    lists), tasks of several graphs interleaved so tiles hold mixed graphs.
+    Integer weights: identical searches. Float weights: above 2048 nodes the
+    two sums run in the same order (identical searches); below, each value is
+    its state's exact value."""
+    from pyqrackising_b200 import _lib
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    O = oracle_mod
+    sizes = [64, 257, 1000, 2100, 3000]
+    Ws = _graphs(kind, sizes, seed=21)
+    bs = BatchedSearch([DeviceGraph(W) for W in Ws], row_lists=False)
+    rng = np.random.default_rng(4)
+    task_graph = [int(g) for g in rng.integers(0, len(sizes), 150)]
+    words = bs.random_states(task_graph, seed=8)
+    for fields in (("f64", "f32") if kind == "float" else ("f64",)):
+        out = {}
+        for on in (1, 0):
+            _lib.call("pqi_batch_set_start_pass", on)
+            try:
+                out[on] = bs.run(task_graph, words, 1, rounds=2, kick=4, seed=3, fields=fields)
+                out[(on, "c")] = bs.cluster_ascent(task_graph, words, 1, cluster_size=4)
+            finally:
+                _lib.call("pqi_batch_set_start_pass", 1)
+        for key in ((1, 0), ((1, "c"), (0, "c"))):
+            a, b = out[key[0]], out[key[1]]
+            if kind == "int":
+                assert torch.equal(a[1], b[1]) and torch.equal(a[0], b[0]) and int(a[2].item()) == int(b[2].item())
+                continue
+            states = bs.unpack(a[1], task_graph)
+            for t, g in enumerate(task_graph):
+                if sizes[g] >= 2048 and fields == "f64":
+                    assert float(a[0][t]) == float(b[0][t])
+                if t % 10 == 0:
+                    assert float(a[0][t]) == pytest.approx(O.compute_energy(states[t], Ws[g]), rel=1e-9, abs=1e-6)
