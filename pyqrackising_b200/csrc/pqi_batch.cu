@@ -135,7 +135,7 @@ __device__ __forceinline__ unsigned long long bmax_key(unsigned long long key) {
 template <typename WT, typename GT, int CH, bool STG, int BT>
 __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k, int xk,
                                                 unsigned long long (*red_key)[8],
-                                                double (*red_g)[8], double (*red_x)[8], int par,
+                                                double (*red_x)[8], int par,
                                                 unsigned long long* out_key, double* out_g,
                                                 double* out_gx) {
   constexpr bool GX = std::is_same<GT, float>::value;
@@ -148,64 +148,55 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   const GT coef = (k >= 0) ? (xk ? (GT)-2 : (GT)2) : (GT)0;
   const WT* __restrict__ row = c.W + (size_t)(k >= 0 ? k : 0) * c.ld;
   float bv = -INFINITY;
-  int bi = -1, bx = 0;
-  double bg = 0.0;
+  int bi = -1;
   // The selection compares gains as float32, lowest node on ties. Per field
   // type the comparison uses as few conversions as give the same result:
   // float fields compare in float (no conversion); int fields compare as int
   // (exact in float below 2^24, more than 127 x the largest n); double fields
-  // round each gain to float once.
+  // round each field to float once (rounding is symmetric, so the gain's
+  // float is +-the field's). Only the best node is kept per thread; its bit
+  // and the winner's exact gain are read back after the selection.
   int bint = INT_MIN;
   constexpr int stride = 4 * BT;  // 4 nodes x BT threads
   // one group of four nodes v0 .. v0 + 3 with their weights of row k
   // (v0 is a multiple of four: node v0 + i sits at fpos(v0) + BT i)
   auto group = [&](int v0, const WT* w4) {
-    if (k >= v0 && k < v0 + 4) c.bits[k >> 5] ^= 1u << (k & 31);
-    const uint32_t word = c.bits[v0 >> 5];
+    if ((unsigned)(k - v0) < 4u) c.bits[k >> 5] ^= 1u << (k & 31);
+    const uint32_t nib = c.bits[v0 >> 5] >> (v0 & 31);  // bits of v0 .. v0 + 3
     GT* const g0 = c.g + fpos<BT>(v0);
+    const bool full = v0 + 3 < n;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-      const int v = v0 + i;
-      if (v < n) {
+      if (full || v0 + i < n) {
         GT y = g0[BT * i];
         if (k >= 0) {
           y += coef * (GT)w4[i];
           g0[BT * i] = y;
         }
-        const int xv = (word >> (v & 31)) & 1;
+        const uint32_t xv = (nib >> i) & 1u;
         if constexpr (GX) {
           // bit k may already be toggled here; W_kk = 0 in the prepared copy
           if (k >= 0) {
-            const float y = xv ? (float)w4[i] : -(float)w4[i];
-            const float t = px_hi + y;
+            const float t0 = xv ? (float)w4[i] : -(float)w4[i];
+            const float t = px_hi + t0;
             const float bb = t - px_hi;
-            px_lo += (px_hi - (t - bb)) + (y - bb);
+            px_lo += (px_hi - (t - bb)) + (t0 - bb);
             px_hi = t;
           }
         }
         // v ascends within a thread: strict '>' keeps the lowest node
-        if constexpr (std::is_same<GT, float>::value) {
-          const float gv = xv ? y : -y;
-          if (gv > bv) {
-            bv = gv;
-            bi = v;
-            bx = xv;
-          }
-        } else if constexpr (std::is_same<GT, int>::value) {
+        if constexpr (std::is_same<GT, int>::value) {
           const int gi = xv ? y : -y;
           if (gi > bint) {
             bint = gi;
-            bi = v;
-            bx = xv;
+            bi = v0 + i;
           }
         } else {
-          const double g = xv ? y : -y;
-          const float gv = (float)g;
+          const float yf = (float)y;
+          const float gv = xv ? yf : -yf;
           if (gv > bv) {
             bv = gv;
-            bi = v;
-            bg = g;
-            bx = xv;
+            bi = v0 + i;
           }
         }
       }
@@ -269,17 +260,13 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
       }
     }
   }
-  if constexpr (std::is_same<GT, float>::value) {
-    bg = (double)bv;
-  } else if constexpr (std::is_same<GT, int>::value) {
-    bv = (float)bint;
-    bg = (double)bint;
-  }
+  if constexpr (std::is_same<GT, int>::value) bv = (float)bint;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // (bit bi is written only by this thread, the owner of node bi)
+  const int bx = bi >= 0 ? (int)((c.bits[bi >> 5] >> (bi & 31)) & 1u) : 0;
   const unsigned long long key = bi >= 0 ? bkey(bv, bi, bx) : 0ull;
   const unsigned long long wk = bmax_key(key);
   if (lane == 0) red_key[par][warp] = wk;
-  if (key != 0ull && key == wk) red_g[par][warp] = bg;
   if constexpr (GX) {
     double px = (double)px_hi + (double)px_lo;
     for (int o = 16; o > 0; o >>= 1) px += __shfl_xor_sync(0xFFFFFFFFu, px, o);
@@ -288,10 +275,17 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
   __syncthreads();
   const int nwarps = blockDim.x >> 5;
   const unsigned long long sk = lane < nwarps ? red_key[par][lane] : 0ull;
-  const double sg = lane < nwarps ? red_g[par][lane] : 0.0;
   const unsigned long long gk = bmax_key(sk);
-  const uint32_t src = __ballot_sync(0xFFFFFFFFu, sk == gk && gk != 0ull);
-  *out_g = __shfl_sync(0xFFFFFFFFu, sg, src ? __ffs(src) - 1 : 0);
+  // the winner's gain from its field: written before the barrier, and a
+  // warp already in the next pass (which flips the winner) leaves it as it
+  // is (W_kk = 0)
+  double g_win = 0.0;
+  if (gk != 0ull) {
+    const int kw = (int)(0x3FFFFFFFu - ((uint32_t)gk >> 1));
+    const double y = (double)c.g[fpos<BT>(kw)];
+    g_win = (gk & 1ull) ? y : -y;
+  }
+  *out_g = g_win;
   *out_key = gk;
   if constexpr (GX) {
     // every warp sums the slots in the same order: one value CTA-wide
@@ -415,7 +409,6 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ double red[32];
   __shared__ unsigned long long red_key[2][8];
-  __shared__ double red_g[2][8];
   __shared__ double red_x[2][8];
   for (int task = blockIdx.x; task < tasks; task += gridDim.x) {
     const BatchGraph G = graphs[task_graph[task]];
@@ -561,7 +554,7 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
     unsigned long long key;
     double gk, gx;
     int par = 0;
-    flip_and_select<WT, GT, CH, STG, BT>(c, -1, 0, red_key, red_g, red_x, par, &key, &gk, &gx);
+    flip_and_select<WT, GT, CH, STG, BT>(c, -1, 0, red_key, red_x, par, &key, &gk, &gx);
     par ^= 1;
     for (int r = 0; r <= rounds; ++r) {
       // steepest ascent: flip the best node while its gain is positive
@@ -580,7 +573,7 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
         bool undone = false;
 #pragma unroll 1
         for (int pass = 0; pass < 2; ++pass) {
-          flip_and_select<WT, GT, CH, STG, BT>(c, k, xk ^ pass, red_key, red_g, red_x, par, &key, &gk, &gx);
+          flip_and_select<WT, GT, CH, STG, BT>(c, k, xk ^ pass, red_key, red_x, par, &key, &gk, &gx);
           par ^= 1;
           if (pass == 1 || !F32 || gx > 0.0) {
             undone = pass == 1;
@@ -613,7 +606,7 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
         const double gp = xp ? (double)c.g[fpos<BT>(pick)] : -(double)c.g[fpos<BT>(pick)];
         __syncthreads();  // everyone has read bit, field and kicked set before they change
         if (threadIdx.x == 0) kicked[pick >> 5] |= 1u << (pick & 31);
-        flip_and_select<WT, GT, CH, STG, BT>(c, pick, xp, red_key, red_g, red_x, par, &key, &gk, &gx);
+        flip_and_select<WT, GT, CH, STG, BT>(c, pick, xp, red_key, red_x, par, &key, &gk, &gx);
         par ^= 1;
         val += scale * (F32 ? gx : gp);  // float64 gain of the kicked node
         ++nflips;
