@@ -274,43 +274,23 @@ __global__ void select_finish_kernel(const unsigned long long* key, SelGeom geo,
 // is float(d) (x2 for a spin glass) and its selection is the maximum 64-bit
 // key (sel_key) over all pairs k < l in k-major order.
 //
-// The upper triangle is cut into tiles of DR rows x (VEC x 256) columns, each
-// W element read once (16-byte loads, VEC consecutive columns per thread);
-// a thread keeps its columns' gains and bits in registers across the tile's
-// rows. Every pair first gets an fp32 estimate a = (f_k + f_l) + c W_kl
-// (f = float(g), c = -2 when the bits agree, else +2). |a - value| is below
-// 2^-22 (|g_k| + |g_l| + |a|), so a pair with a < thr - delta,
+// The upper triangle is cut into tiles of DR rows x CW columns (CW = 2048
+// float32 or 8192 int8 columns: 8 KB of each row), each W element read once.
+// Every pair first gets an fp32 estimate a = f_k + f_l + c W_kl (f = the gain
+// in the estimate's type, c = -2 when the bits agree, else +2). |a - value|
+// is below 2^-22 (|g_k| + |g_l| + |a|), so a pair with a < thr - delta,
 // delta = 2^-20 (max|g_k| + max|g_l| + |thr|), has value < thr; thr is a value
 // some selectable pair (key != 0) reaches, so such a pair cannot be the
-// maximum and is skipped. Only the remaining pairs - the first ones a thread
-// meets, then the rare near-maxima - take the exact float64 value and key.
-// thr is shared per block (shared memory) and across blocks (one global
-// word), both as order-preserving uint32 under atomicMax.
+// maximum and is skipped. Only tiles holding a pair at the cut - the rare
+// near-maxima - take pairs' exact float64 values and keys. thr is shared per
+// block (shared memory) and across blocks (one global word), both as
+// order-preserving uint32 under atomicMax, and seeded before the pass.
 
-constexpr int DR = 8;                 // rows per tile
-constexpr int DTHREADS = 256;
-
-template <typename WT>
-struct DoubleVec {
-  static constexpr int VEC = sizeof(WT) == 4 ? 4 : 16;  // columns per thread (16 bytes)
-};
+constexpr int DR = 8;  // rows per tile
 
 __device__ __forceinline__ float thr_of(uint32_t o) {
   // ordered 0 (nothing published yet) and anything below -inf read as -inf
   return o < ord_f32(-INFINITY) ? -INFINITY : unord_f32(o);
-}
-
-// The gains in the estimate's type, converted once per pass: float32 for float
-// weights, int32 (exact) for int8 weights.
-template <typename ET>
-__global__ void gains_to_estimate_kernel(const double* __restrict__ g64, int n, ET* __restrict__ out) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if constexpr (std::is_same<ET, float>::value) {
-      out[i] = (float)g64[i];
-    } else {
-      out[i] = (int)llrint(g64[i]);
-    }
-  }
 }
 
 // Tie priority of pair index c under the reference geometry, from (t, j) =
@@ -322,157 +302,57 @@ __device__ __forceinline__ uint64_t pair_key(float v, uint32_t t, uint32_t j, co
   return ((uint64_t)ord_f32(v) << 32) | (uint64_t)(0xFFFFFFFFu - ((grp * geo.L + r) * geo.J + j));
 }
 
+// Before the pass: the gains in the estimate's type (float32 for float
+// weights, int32 - exact - for int8 weights), and a first threshold: pair
+// (k, k + 1) of every k taken exactly, its key folded into the result and,
+// when selectable, its value into the shared threshold (one atomic per warp),
+// so that no tile starts from an empty threshold.
 template <typename WT>
-__global__ void __launch_bounds__(DTHREADS) double_tile_kernel(
-    const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
-    const double* __restrict__ g64, const void* __restrict__ gest_v, int spin, SelGeom geo,
-    unsigned long long* key, unsigned int* gthr) {
-  constexpr int VEC = DoubleVec<WT>::VEC;
-  constexpr int CW = VEC * DTHREADS;  // columns per tile
+__global__ void double_prep_kernel(const WT* __restrict__ Wp, int ld, int n,
+                                   const uint32_t* __restrict__ theta,
+                                   const double* __restrict__ g64, int spin, SelGeom geo,
+                                   void* __restrict__ gest_v, unsigned long long* key,
+                                   unsigned int* gthr) {
   constexpr bool INT = sizeof(WT) == 1;
-  // the pair estimate's type: exact int32 for int8 weights, float32 otherwise
-  typedef typename std::conditional<INT, int, float>::type ET;
-  const ET* __restrict__ gest = static_cast<const ET*>(gest_v);
-  __shared__ uint64_t scratch[32];
-  __shared__ unsigned int s_thr;
-  if (threadIdx.x == 0) s_thr = 0u;
-  __syncthreads();
-  // tiles (row group rg, column chunk c) in a rectangle walked with a stride of
-  // gridDim.x, advanced without divisions; tiles wholly at or below the
-  // diagonal are skipped
-  const int ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
-  const int nc = (n + CW - 1) / CW;      // column chunks
-  const int dstep_rg = (int)(gridDim.x / nc), dstep_c = (int)(gridDim.x - (gridDim.x / nc) * nc);
-  int rg = (int)(blockIdx.x / nc), c = (int)(blockIdx.x - (blockIdx.x / nc) * nc);
-  uint64_t best = 0;
-  float thr = -INFINITY;
-  for (; rg < ng; rg += dstep_rg, c += dstep_c) {
-    if (c >= nc) {
-      c -= nc;
-      ++rg;
-      if (rg >= ng) break;
-    }
-    if ((c + 1) * CW <= rg * DR + 1) continue;  // every column <= every row's k
-    const int k0 = rg * DR;
-    const int l0 = c * CW + threadIdx.x * VEC;
-    // the tile's rows: gains and bits (the same for every thread)
-    ET fk[DR];
-    uint32_t xk = 0;
-    float gt = 0.0f;
-#pragma unroll
-    for (int i = 0; i < DR; ++i) {
-      const int k = min(k0 + i, n - 1);
-      fk[i] = __ldg(gest + k);
-      if constexpr (!INT) gt = fmaxf(gt, fabsf(fk[i]));
-      xk |= (uint32_t)get_bit32(theta, k) << i;
-    }
-    // this thread's columns
-    ET fl[VEC];
-    float flmax = 0.0f;
-    const uint32_t lw = l0 < n ? __ldg(theta + (l0 >> 5)) >> (l0 & 31) : 0u;
-#pragma unroll
-    for (int e = 0; e < VEC; ++e) {
-      const int l = l0 + e;
-      fl[e] = l < n ? __ldg(gest + l) : ET(0);
-      if constexpr (!INT) flmax = fmaxf(flmax, fabsf(fl[e]));
-    }
-    // every row's W slice in flight before any is used (l0 < n keeps the
-    // 16-byte load inside the padded row of ld >= n elements)
-    WT w[DR][VEC];
-#pragma unroll
-    for (int i = 0; i < DR; ++i) {
-      const int k = min(k0 + i, n - 1);
-      if (l0 < n) {
-        const int4 v = __ldg(reinterpret_cast<const int4*>(Wp + (size_t)k * ld + l0));
-        memcpy(&w[i][0], &v, 16);
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+    const int k = base + (int)threadIdx.x;
+    uint64_t kk = 0;
+    unsigned int o = 0;
+    if (k < n) {
+      const double gk = g64[k];
+      if constexpr (INT) {
+        static_cast<int*>(gest_v)[k] = (int)llrint(gk);
       } else {
-#pragma unroll
-        for (int e = 0; e < VEC; ++e) w[i][e] = (WT)0;
+        static_cast<float*>(gest_v)[k] = (float)gk;
       }
-    }
-    thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(gthr))));
-    // the skip bound: 2^-20 (max |g_k| + max |g_l| + |thr|) for float
-    // estimates, none for exact integer ones
-    const float base = gt + flmax;
-    float cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
-    // integer estimates compare as integers (thr is then an integer value)
-    int cut_i = thr > -INFINITY ? (int)thr : INT_MIN;
-    // 1. the estimates of the thread's DR x VEC pairs (unrolled, registers
-    // only): does any reach the cut? a = f_k + f_l + 2 (-/+ W): W's sign is
-    // flipped where bits k and l agree (one three-way XOR per pair)
-    bool any = false;
-#pragma unroll
-    for (int i = 0; i < DR; ++i) {
-      const uint32_t xki = (xk >> i) & 1u;
-#pragma unroll
-      for (int e = 0; e < VEC; ++e) {
-        const uint32_t xle = (lw >> e) & 1u;
-        if constexpr (INT) {
-          const int m = -(int)(xki ^ xle);  // 0 where the bits agree, else -1
-          const int wi = (int)w[i][e];
-          any |= fk[i] + fl[e] - 2 * ((wi ^ m) - m) >= cut_i;
-        } else {
-          const float cw =
-              __uint_as_float(__float_as_uint(w[i][e]) ^ ((xki ^ xle ^ 1u) << 31));
-          any |= fmaf(2.0f, cw, fk[i] + fl[e]) >= cut;
-        }
-      }
-    }
-    // 2. a tile with a pair at the cut (rare once the threshold has risen):
-    // every pair again in one code path (not unrolled), its estimate against
-    // the cut as it rises, then the exact value and key. The operands come
-    // back from L1 (this tile's loads).
-    if (any) {
-#pragma unroll 1
-      for (int b = 0; b < DR * VEC; ++b) {
-        const int i = b / VEC, e = b % VEC;
-        const int k = k0 + i, l = l0 + e;
-        if (k >= n - 1 || l <= k || l >= n) continue;
-        const WT wv = __ldg(Wp + (size_t)k * ld + l);
-        const uint32_t flip = (uint32_t)(get_bit32(theta, (uint32_t)k) ^ get_bit32(theta, (uint32_t)l)) ^ 1u;
-        float v;
-        if constexpr (INT) {
-          const int ai = __ldg(gest + k) + __ldg(gest + l) + (flip ? -2 * (int)wv : 2 * (int)wv);
-          if (ai < cut_i) continue;
-          v = (float)ai;  // below 2^24 in magnitude: exact
-        } else {
-          const float cw = __uint_as_float(__float_as_uint(wv) ^ (flip << 31));
-          if (fmaf(2.0f, cw, __ldg(gest + k) + __ldg(gest + l)) < cut) continue;
-          const double wd = (double)wv;
-          v = (float)(__ldg(g64 + k) + __ldg(g64 + l) - (flip ? 2.0 * wd : -2.0 * wd));
-        }
+      if (k + 1 < n) {
+        const int l = k + 1;
+        const double wd = (double)Wp[(size_t)k * ld + l];
+        const bool agree = get_bit32(theta, (uint32_t)k) == get_bit32(theta, (uint32_t)l);
+        float v = (float)(gk + g64[l] - (agree ? 2.0 * wd : -2.0 * wd));
         const float vu = v;
         if (spin) v *= 2.0f;
-        const uint32_t c = (uint32_t)(pair_base(k, n) + (long long)(l - k - 1));
-        const uint64_t kk = pair_key(v, c % geo.G, c / geo.G, geo);
-        best = kk > best ? kk : best;
-        if (kk != 0ull && vu > thr) {
-          thr = vu;
-          cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
-          cut_i = (int)thr;
-        }
+        const uint32_t c = (uint32_t)pair_base(k, n);  // pair (k, k + 1)
+        kk = pair_key(v, c % geo.G, c / geo.G, geo);
+        if (kk != 0ull) o = ord_f32(vu);
       }
     }
-    // publish this thread's threshold (a value a selectable pair reaches)
-    if (thr > -INFINITY) {
-      const unsigned int o = ord_f32(thr);
-      if (o > *(volatile unsigned int*)&s_thr) {
-        atomicMax(&s_thr, o);
-        if (o > __ldcg(gthr)) atomicMax(gthr, o);
-      }
+    kk = warp_max_u64(kk);
+    o = __reduce_max_sync(0xFFFFFFFFu, o);
+    if ((threadIdx.x & 31) == 0) {
+      if (kk) atomicMax(key, (unsigned long long)kk);
+      if (o) atomicMax(gthr, o);
     }
   }
-  best = block_max_u64(best, scratch);
-  if (threadIdx.x == 0 && best) atomicMax(key, (unsigned long long)best);
 }
 
-// ---------------------------------------------------------------------------
 // The same pass with W streamed through shared memory: one persistent CTA per
 // SM, a producer warp copying each tile's DR row segments of DS_ROW_BYTES
 // (cp.async.bulk, completion counted on the stage's mbarrier) into a ring of
 // DS_STAGES stages, and DS_CONSUMERS threads that score the tile from shared
-// memory (the estimate pass, then the exact path for flagged tiles, as in
-// double_tile_kernel) and release the stage. The copies run up to
+// memory (the estimate pass, then the exact path for flagged tiles) and
+// release the stage. The copies run up to
 // DS_STAGES tiles ahead of the scoring, so HBM sees a deep queue of large
 // requests whatever the scoring's latency.
 constexpr int DS_STAGES = 3;
@@ -491,6 +371,18 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
       : "memory");
 }
 
+// A stage's tile header, written by the producer warp before the stage's
+// copies are armed (the arrive releases it to the consumers): the tile's
+// first row (-1 ends the walk), column chunk, the rows' estimate gains and
+// bits, and the largest |row gain|.
+template <typename ET>
+struct DsTile {
+  int k0, c;
+  uint32_t xk;
+  float gt;
+  ET fk[DR];
+};
+
 template <typename WT>
 __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
     const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
@@ -504,6 +396,7 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
   extern __shared__ __align__(1024) unsigned char ring[];
   __shared__ __align__(8) uint64_t full_bar[DS_STAGES];
   __shared__ __align__(8) uint64_t empty_bar[DS_STAGES];
+  __shared__ DsTile<ET> meta[DS_STAGES];
   __shared__ uint64_t scratch[32];
   __shared__ unsigned int s_thr;
   __shared__ int s_fail;
@@ -519,24 +412,57 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
     s_fail = 0;
   }
   __syncthreads();
-  const int ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
-  const int nc = (n + CW - 1) / CW;      // column chunks
-  const int total = ng * nc;  // (n <= 46341: well inside int)
   uint64_t best = 0;
   if (warp == DS_CONSUMERS / 32) {
-    // producer: the tiles of this CTA in order, each into the next stage once
-    // the consumers have released that stage's previous tile
-    if (lane == 0) {
-      int it = 0;
-      for (int tau = blockIdx.x; tau < total; tau += gridDim.x) {
-        const int rg = tau / nc, c = tau - (tau / nc) * nc;
-        if ((c + 1) * CW <= rg * DR + 1) continue;  // wholly at or below the diagonal
-        const int st = it % DS_STAGES;
-        const uint32_t use = (uint32_t)(it / DS_STAGES);
-        if (use > 0 && !tc::mbar_wait(&empty_bar[st], (use - 1) & 1u)) {
-          s_fail = 1;
-          break;
+    // producer: walks this CTA's tiles (a stride of gridDim.x over the
+    // rectangle of row groups x column chunks, tiles wholly at or below the
+    // diagonal skipped), writes each tile's header and arms its copies once
+    // the consumers have released the stage; a header with k0 = -1 ends
+    const int ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
+    const int nc = (n + CW - 1) / CW;      // column chunks
+    const int total = ng * nc;             // (n <= 46341: well inside int)
+    int it = 0;
+    for (int tau = blockIdx.x;; tau += gridDim.x) {
+      int rg = 0, c = 0;
+      bool end = tau >= total;
+      if (!end) {
+        rg = tau / nc;
+        c = tau - rg * nc;
+        if ((c + 1) * CW <= rg * DR + 1) continue;
+      }
+      const int st = it % DS_STAGES;
+      const uint32_t use = (uint32_t)(it / DS_STAGES);
+      if (use > 0 && !tc::mbar_wait_warp(&empty_bar[st], (use - 1) & 1u)) {
+        s_fail = 1;
+        break;
+      }
+      DsTile<ET>& m = meta[st];
+      if (end) {
+        if (lane == 0) {
+          m.k0 = -1;
+          tc::mbar_arrive(&full_bar[st]);
         }
+        break;
+      }
+      const int k0 = rg * DR;
+      {
+        const int k = min(k0 + lane, n - 1);
+        const ET fv = lane < DR ? __ldg(gest + k) : ET(0);
+        const uint32_t bit = lane < DR ? (uint32_t)get_bit32(theta, (uint32_t)k) : 0u;
+        const uint32_t xk = __ballot_sync(0xFFFFFFFFu, bit != 0u);
+        float a = fabsf((float)fv);
+#pragma unroll
+        for (int o = 1; o < DR; o <<= 1) a = fmaxf(a, __shfl_xor_sync(0xFFFFFFFFu, a, o));
+        if (lane < DR) m.fk[lane] = fv;
+        if (lane == 0) {
+          m.k0 = k0;
+          m.c = c;
+          m.xk = xk;
+          m.gt = a;
+        }
+      }
+      __syncwarp();
+      if (lane == 0) {
         // the row segments: up to CW columns, within the padded row (ld is a
         // multiple of 128, so the size is a multiple of 512 bytes)
         const int col0 = c * CW;
@@ -545,35 +471,31 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
         unsigned char* dst = ring + (size_t)st * DS_TILE_BYTES;
 #pragma unroll
         for (int i = 0; i < DR; ++i) {
-          const int k = min(rg * DR + i, n - 1);
+          const int k = min(k0 + i, n - 1);
           bulk_copy_g2s(dst + i * DS_ROW_BYTES, Wp + (size_t)k * ld + col0, bytes, &full_bar[st]);
         }
-        ++it;
       }
+      ++it;
     }
   } else {
     float thr = -INFINITY;
-    int it = 0;
-    for (int tau = blockIdx.x; tau < total; tau += gridDim.x) {
-      const int rg = tau / nc, c = tau - (tau / nc) * nc;
-      if ((c + 1) * CW <= rg * DR + 1) continue;
+    for (int it = 0;; ++it) {
       const int st = it % DS_STAGES;
       const uint32_t use = (uint32_t)(it / DS_STAGES);
-      ++it;
-      const int k0 = rg * DR;
-      const int l0 = c * CW + (int)threadIdx.x * VEC;
-      // the tile's rows: gains and bits (the same for every thread), this
-      // thread's columns: loaded while the stage's copies land
-      ET fk[DR];
-      uint32_t xk = 0;
-      float gt = 0.0f;
-#pragma unroll
-      for (int i = 0; i < DR; ++i) {
-        const int k = min(k0 + i, n - 1);
-        fk[i] = __ldg(gest + k);
-        if constexpr (!INT) gt = fmaxf(gt, fabsf(fk[i]));
-        xk |= (uint32_t)get_bit32(theta, k) << i;
+      thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(gthr))));
+      if (!tc::mbar_wait_warp(&full_bar[st], use & 1u)) {
+        s_fail = 1;
+        break;
       }
+      const DsTile<ET>& m = meta[st];
+      const int k0 = m.k0;
+      if (k0 < 0) break;
+      const int c = m.c;
+      const uint32_t xk = m.xk;
+      ET fk[DR];
+#pragma unroll
+      for (int i = 0; i < DR; ++i) fk[i] = m.fk[i];
+      const int l0 = c * CW + (int)threadIdx.x * VEC;
       ET fl[VEC];
       float flmax = 0.0f;
       const uint32_t lw = l0 < n ? __ldg(theta + (l0 >> 5)) >> (l0 & 31) : 0u;
@@ -583,11 +505,6 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
         fl[e] = l < n ? __ldg(gest + l) : ET(0);
         if constexpr (!INT) flmax = fmaxf(flmax, fabsf(fl[e]));
       }
-      thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(gthr))));
-      if (!tc::mbar_wait_warp(&full_bar[st], use & 1u)) {
-        s_fail = 1;
-        break;
-      }
       const unsigned char* tile = ring + (size_t)st * DS_TILE_BYTES + threadIdx.x * 16;
       WT w[DR][VEC];
 #pragma unroll
@@ -595,11 +512,11 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
         const int4 v = *reinterpret_cast<const int4*>(tile + i * DS_ROW_BYTES);
         memcpy(&w[i][0], &v, 16);
       }
-      const float base = gt + flmax;
+      const float base = m.gt + flmax;
       float cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
       int cut_i = thr > -INFINITY ? (int)thr : INT_MIN;
       // (columns past the copied row segment hold stale bytes: such a thread
-      // has no column below n and skips the estimates)
+      // has no column below n and skips the exact path)
       bool any = false;
       if constexpr (INT) {
 #pragma unroll
@@ -607,9 +524,9 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
           const uint32_t xki = (xk >> i) & 1u;
 #pragma unroll
           for (int e = 0; e < VEC; ++e) {
-            const int m = -(int)(xki ^ ((lw >> e) & 1u));
+            const int mm = -(int)(xki ^ ((lw >> e) & 1u));
             const int wi = (int)w[i][e];
-            any |= fk[i] + fl[e] - 2 * ((wi ^ m) - m) >= cut_i;
+            any |= fk[i] + fl[e] - 2 * ((wi ^ mm) - mm) >= cut_i;
           }
         }
       } else {
@@ -643,8 +560,7 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
           const int k = k0 + i, l = l0 + e;
           if (k >= n - 1 || l <= k || l >= n) continue;
           const WT wv = tw[i * (DS_ROW_BYTES / (int)sizeof(WT)) + (l - c * CW)];
-          const uint32_t flip =
-              (uint32_t)(get_bit32(theta, (uint32_t)k) ^ get_bit32(theta, (uint32_t)l)) ^ 1u;
+          const uint32_t flip = (((xk >> i) & 1u) ^ ((lw >> e) & 1u)) ^ 1u;
           float v;
           if constexpr (INT) {
             const int ai = __ldg(gest + k) + __ldg(gest + l) + (flip ? -2 * (int)wv : 2 * (int)wv);
@@ -1032,11 +948,13 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
   void* gest = ws.take<float>(n);
   PQI_CHECK_ARG(gest);
   if (w->kind == PQI_W_I8) {
-    gains_to_estimate_kernel<int><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(gains64, n, static_cast<int*>(gest));
+    double_prep_kernel<int8_t><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(
+        w->W_i8, w->ld, n, theta, gains64, is_spin_glass, geo, gest, key, gthr);
   } else {
-    gains_to_estimate_kernel<float><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(gains64, n, static_cast<float*>(gest));
+    double_prep_kernel<float><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(
+        w->W_f32z, w->ld, n, theta, gains64, is_spin_glass, geo, gest, key, gthr);
   }
-  PQI_LAUNCHED("gains_to_estimate_kernel");
+  PQI_LAUNCHED("double_prep_kernel");
   // one persistent CTA per SM (the stage ring takes most of shared memory)
   static int sms = 0;
   static bool attr_set[2] = {false, false};
