@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(256) start_fields_kernel(
 // BT: threads per CTA (256; 128 or 64 for small graphs: two or four times the
 // resident tasks per SM, at the same registers per thread).
 template <typename WT, int CH, bool F32, bool STG, int BT>
-__global__ void __launch_bounds__(BT, (F32 ? 4 : (CH > 4 ? 2 : 3)) * 256 / BT) batch_search_kernel(
+__global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_kernel(
     const BatchGraph* __restrict__ graphs, const int* __restrict__ task_graph,
     const uint32_t* __restrict__ init_states, int words_pitch, int tasks, int spin, int rounds,
     int kick, int flip_budget, uint64_t seed, const double* __restrict__ kick_cdf,
@@ -998,11 +998,8 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   } else {
     if (groups <= 2) {
       PQI_BATCH_LAUNCH(float, 2, false, false, 256);
-    } else if (groups <= 4) {
-      PQI_BATCH_LAUNCH(float, 4, false, false, 256);
     } else {
-      // every row group of a pass in flight at once (one wait per flip)
-      PQI_BATCH_LAUNCH(float, 8, false, false, 256);
+      PQI_BATCH_LAUNCH(float, 4, false, false, 256);
     }
   }
 #undef PQI_BATCH_LAUNCH
