@@ -303,47 +303,68 @@ __device__ __forceinline__ uint64_t pair_key(float v, uint32_t t, uint32_t j, co
 }
 
 // Before the pass: the gains in the estimate's type (float32 for float
-// weights, int32 - exact - for int8 weights), and a first threshold: pair
-// (k, k + 1) of every k taken exactly, its key folded into the result and,
-// when selectable, its value into the shared threshold (one atomic per warp),
-// so that no tile starts from an empty threshold.
+// weights, int32 - exact - for int8 weights), and a first threshold close to
+// the maximum: the node m of the largest gain (grid-wide, then the last
+// block to finish) takes every pair (k, m) exactly, folds their keys into the
+// result and the largest selectable value into the shared threshold - the
+// best pairs usually contain the best single node, so few tiles then hold a
+// pair at the cut. ctl: [0] the argmax key, [1] the block counter (zeroed
+// with the result).
 template <typename WT>
-__global__ void double_prep_kernel(const WT* __restrict__ Wp, int ld, int n,
-                                   const uint32_t* __restrict__ theta,
-                                   const double* __restrict__ g64, int spin, SelGeom geo,
-                                   void* __restrict__ gest_v, unsigned long long* key,
-                                   unsigned int* gthr) {
+__global__ void __launch_bounds__(256) double_prep_kernel(
+    const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
+    const double* __restrict__ g64, int spin, SelGeom geo, void* __restrict__ gest_v,
+    unsigned long long* key, unsigned int* gthr, unsigned long long* ctl) {
   constexpr bool INT = sizeof(WT) == 1;
-  const int stride = gridDim.x * blockDim.x;
-  for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
-    const int k = base + (int)threadIdx.x;
-    uint64_t kk = 0;
-    unsigned int o = 0;
-    if (k < n) {
-      const double gk = g64[k];
-      if constexpr (INT) {
-        static_cast<int*>(gest_v)[k] = (int)llrint(gk);
-      } else {
-        static_cast<float*>(gest_v)[k] = (float)gk;
-      }
-      if (k + 1 < n) {
-        const int l = k + 1;
-        const double wd = (double)Wp[(size_t)k * ld + l];
-        const bool agree = get_bit32(theta, (uint32_t)k) == get_bit32(theta, (uint32_t)l);
-        float v = (float)(gk + g64[l] - (agree ? 2.0 * wd : -2.0 * wd));
-        const float vu = v;
-        if (spin) v *= 2.0f;
-        const uint32_t c = (uint32_t)pair_base(k, n);  // pair (k, k + 1)
-        kk = pair_key(v, c % geo.G, c / geo.G, geo);
-        if (kk != 0ull) o = ord_f32(vu);
-      }
+  __shared__ uint64_t scratch[32];
+  __shared__ unsigned int s_last;
+  uint64_t am = 0;  // ordered float gain << 32 | (0xFFFFFFFF - node): largest gain, lowest node
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const double gk = g64[k];
+    if constexpr (INT) {
+      static_cast<int*>(gest_v)[k] = (int)llrint(gk);
+    } else {
+      static_cast<float*>(gest_v)[k] = (float)gk;
     }
-    kk = warp_max_u64(kk);
-    o = __reduce_max_sync(0xFFFFFFFFu, o);
-    if ((threadIdx.x & 31) == 0) {
-      if (kk) atomicMax(key, (unsigned long long)kk);
-      if (o) atomicMax(gthr, o);
+    const uint64_t a = ((uint64_t)ord_f32((float)gk) << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)k);
+    am = a > am ? a : am;
+  }
+  am = block_max_u64(am, scratch);
+  if (threadIdx.x == 0) {
+    if (am) atomicMax(ctl, (unsigned long long)am);
+    __threadfence();
+    s_last = atomicAdd(reinterpret_cast<unsigned int*>(ctl + 1), 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const uint64_t top = *(volatile unsigned long long*)ctl;
+  if (!top) return;
+  const int m = (int)(0xFFFFFFFFu - (uint32_t)top);
+  const uint32_t xm = (uint32_t)get_bit32(theta, (uint32_t)m);
+  uint64_t kk_best = 0;
+  unsigned int o_best = 0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    if (k == m) continue;
+    const int a = min(k, m), b = max(k, m);
+    const double wd = (double)Wp[(size_t)a * ld + b];
+    const bool agree = (uint32_t)get_bit32(theta, (uint32_t)k) == xm;
+    float v = (float)(g64[a] + g64[b] - (agree ? 2.0 * wd : -2.0 * wd));
+    const float vu = v;
+    if (spin) v *= 2.0f;
+    const uint32_t c = (uint32_t)(pair_base(a, n) + (long long)(b - a - 1));
+    const uint64_t kk = pair_key(v, c % geo.G, c / geo.G, geo);
+    kk_best = kk > kk_best ? kk : kk_best;
+    if (kk != 0ull) {
+      const unsigned int o = ord_f32(vu);
+      o_best = o > o_best ? o : o_best;
     }
+  }
+  kk_best = block_max_u64(kk_best, scratch);
+  const unsigned int o_all = (unsigned int)(block_max_u64(o_best, scratch));
+  if (threadIdx.x == 0) {
+    if (kk_best) atomicMax(key, (unsigned long long)kk_best);
+    if (o_all) atomicMax(gthr, o_all);
   }
 }
 
@@ -518,6 +539,7 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
       // (columns past the copied row segment hold stale bytes: such a thread
       // has no column below n and skips the exact path)
       bool any = false;
+      float ra[DR];  // float: each row's largest estimate
       if constexpr (INT) {
 #pragma unroll
         for (int i = 0; i < DR; ++i) {
@@ -538,7 +560,6 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
         uint32_t cm[VEC];
 #pragma unroll
         for (int e = 0; e < VEC; ++e) cm[e] = ((lw >> e) & 1u) << 31;
-        float amax = -INFINITY;
 #pragma unroll
         for (int i = 0; i < DR; ++i) {
           const uint32_t rm = (((xk >> i) & 1u) ^ 1u) << 31;
@@ -548,15 +569,29 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
             const float cw = __uint_as_float(__float_as_uint(w[i][e]) ^ rm ^ cm[e]);
             r = fmaxf(r, fmaf(2.0f, cw, fl[e]));
           }
-          amax = fmaxf(amax, fk[i] + r);
+          ra[i] = fk[i] + r;
         }
+        float amax = ra[0];
+#pragma unroll
+        for (int i = 1; i < DR; ++i) amax = fmaxf(amax, ra[i]);
         any = amax >= cut;
       }
       if (any && l0 < n) {
         const WT* tw = reinterpret_cast<const WT*>(ring + (size_t)st * DS_TILE_BYTES);
+        // float: only the rows whose largest estimate reaches the cut
+        uint32_t rows = (1u << DR) - 1u;
+        if constexpr (!INT) {
+          rows = 0u;
+#pragma unroll
+          for (int i = 0; i < DR; ++i) rows |= (uint32_t)(ra[i] >= cut) << i;
+        }
 #pragma unroll 1
         for (int b = 0; b < DR * VEC; ++b) {
           const int i = b / VEC, e = b % VEC;
+          if (!((rows >> i) & 1u)) {
+            b += VEC - 1 - e;  // the rest of the row
+            continue;
+          }
           const int k = k0 + i, l = l0 + e;
           if (k >= n - 1 || l <= k || l >= n) continue;
           const WT wv = tw[i * (DS_ROW_BYTES / (int)sizeof(WT)) + (l - c * CW)];
@@ -931,7 +966,8 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
   SelGeom geo;
   PQI_CHECK_ARG(make_sel_geom(combo, global_size, local_size, &geo));
   Workspace ws(workspace, workspace_bytes);
-  unsigned long long* key = ws.take<unsigned long long>(2);  // key, then the threshold word
+  // key, the threshold word, then the prep kernel's argmax key and block counter
+  unsigned long long* key = ws.take<unsigned long long>(4);
   PQI_CHECK_ARG(key);
   cudaStream_t s = as_stream(stream);
   if (!gains64) {
@@ -941,18 +977,19 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     if (rc) return rc;
     gains64 = g;
   }
-  // key (8 bytes) and the shared threshold (4 bytes), zeroed together
-  PQI_TRY(cudaMemsetAsync(key, 0, 16, s));
+  // key (8 bytes), the shared threshold (4 bytes) and the prep kernel's
+  // argmax and counter, zeroed together
+  PQI_TRY(cudaMemsetAsync(key, 0, 32, s));
   unsigned int* gthr = reinterpret_cast<unsigned int*>(key + 1);
   // the gains in the estimate's type (4 bytes each)
   void* gest = ws.take<float>(n);
   PQI_CHECK_ARG(gest);
   if (w->kind == PQI_W_I8) {
     double_prep_kernel<int8_t><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(
-        w->W_i8, w->ld, n, theta, gains64, is_spin_glass, geo, gest, key, gthr);
+        w->W_i8, w->ld, n, theta, gains64, is_spin_glass, geo, gest, key, gthr, key + 2);
   } else {
     double_prep_kernel<float><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(
-        w->W_f32z, w->ld, n, theta, gains64, is_spin_glass, geo, gest, key, gthr);
+        w->W_f32z, w->ld, n, theta, gains64, is_spin_glass, geo, gest, key, gthr, key + 2);
   }
   PQI_LAUNCHED("double_prep_kernel");
   // one persistent CTA per SM (the stage ring takes most of shared memory)
