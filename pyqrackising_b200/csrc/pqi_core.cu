@@ -303,22 +303,15 @@ __device__ __forceinline__ uint64_t pair_key(float v, uint32_t t, uint32_t j, co
 }
 
 // Before the pass: the gains in the estimate's type (float32 for float
-// weights, int32 - exact - for int8 weights), and a first threshold close to
-// the maximum: the node m of the largest gain (grid-wide, then the last
-// block to finish) takes every pair (k, m) exactly, folds their keys into the
-// result and the largest selectable value into the shared threshold - the
-// best pairs usually contain the best single node, so few tiles then hold a
-// pair at the cut. ctl: [0] the argmax key, [1] the block counter (zeroed
-// with the result).
+// weights, int32 - exact - for int8 weights) and the node m of the largest
+// gain (ctl[0]: ordered gain << 32 | ~node, so the lowest node on ties).
 template <typename WT>
-__global__ void __launch_bounds__(256) double_prep_kernel(
-    const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
-    const double* __restrict__ g64, int spin, SelGeom geo, void* __restrict__ gest_v,
-    unsigned long long* key, unsigned int* gthr, unsigned long long* ctl) {
+__global__ void __launch_bounds__(256) double_prep_kernel(const double* __restrict__ g64, int n,
+                                                          void* __restrict__ gest_v,
+                                                          unsigned long long* ctl) {
   constexpr bool INT = sizeof(WT) == 1;
   __shared__ uint64_t scratch[32];
-  __shared__ unsigned int s_last;
-  uint64_t am = 0;  // ordered float gain << 32 | (0xFFFFFFFF - node): largest gain, lowest node
+  uint64_t am = 0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const double gk = g64[k];
     if constexpr (INT) {
@@ -330,41 +323,44 @@ __global__ void __launch_bounds__(256) double_prep_kernel(
     am = a > am ? a : am;
   }
   am = block_max_u64(am, scratch);
-  if (threadIdx.x == 0) {
-    if (am) atomicMax(ctl, (unsigned long long)am);
-    __threadfence();
-    s_last = atomicAdd(reinterpret_cast<unsigned int*>(ctl + 1), 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  const uint64_t top = *(volatile unsigned long long*)ctl;
+  if (threadIdx.x == 0 && am) atomicMax(ctl, (unsigned long long)am);
+}
+
+// A first threshold close to the maximum: every pair (k, m) with the node m
+// of the largest gain taken exactly - the best pairs usually contain the
+// best single node, so few tiles then hold a pair at the cut. Their keys go
+// into the result, the largest selectable value into the shared threshold
+// (one atomic per warp).
+template <typename WT>
+__global__ void __launch_bounds__(256) double_seed_kernel(
+    const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
+    const double* __restrict__ g64, int spin, SelGeom geo, const unsigned long long* ctl,
+    unsigned long long* key, unsigned int* gthr) {
+  const uint64_t top = *ctl;
   if (!top) return;
   const int m = (int)(0xFFFFFFFFu - (uint32_t)top);
   const uint32_t xm = (uint32_t)get_bit32(theta, (uint32_t)m);
-  uint64_t kk_best = 0;
-  unsigned int o_best = 0;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) {
-    if (k == m) continue;
-    const int a = min(k, m), b = max(k, m);
-    const double wd = (double)Wp[(size_t)a * ld + b];
-    const bool agree = (uint32_t)get_bit32(theta, (uint32_t)k) == xm;
-    float v = (float)(g64[a] + g64[b] - (agree ? 2.0 * wd : -2.0 * wd));
-    const float vu = v;
-    if (spin) v *= 2.0f;
-    const uint32_t c = (uint32_t)(pair_base(a, n) + (long long)(b - a - 1));
-    const uint64_t kk = pair_key(v, c % geo.G, c / geo.G, geo);
-    kk_best = kk > kk_best ? kk : kk_best;
-    if (kk != 0ull) {
-      const unsigned int o = ord_f32(vu);
-      o_best = o > o_best ? o : o_best;
+  for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+    const int k = base + (int)threadIdx.x;
+    uint64_t kk = 0;
+    unsigned int o = 0;
+    if (k < n && k != m) {
+      const int a = min(k, m), b = max(k, m);
+      const double wd = (double)Wp[(size_t)a * ld + b];
+      const bool agree = (uint32_t)get_bit32(theta, (uint32_t)k) == xm;
+      float v = (float)(g64[a] + g64[b] - (agree ? 2.0 * wd : -2.0 * wd));
+      const float vu = v;
+      if (spin) v *= 2.0f;
+      const uint32_t c = (uint32_t)(pair_base(a, n) + (long long)(b - a - 1));
+      kk = pair_key(v, c % geo.G, c / geo.G, geo);
+      if (kk != 0ull) o = ord_f32(vu);
     }
-  }
-  kk_best = block_max_u64(kk_best, scratch);
-  const unsigned int o_all = (unsigned int)(block_max_u64(o_best, scratch));
-  if (threadIdx.x == 0) {
-    if (kk_best) atomicMax(key, (unsigned long long)kk_best);
-    if (o_all) atomicMax(gthr, o_all);
+    kk = warp_max_u64(kk);
+    o = __reduce_max_sync(0xFFFFFFFFu, o);
+    if ((threadIdx.x & 31) == 0) {
+      if (kk) atomicMax(key, (unsigned long long)kk);
+      if (o) atomicMax(gthr, o);
+    }
   }
 }
 
@@ -966,8 +962,8 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
   SelGeom geo;
   PQI_CHECK_ARG(make_sel_geom(combo, global_size, local_size, &geo));
   Workspace ws(workspace, workspace_bytes);
-  // key, the threshold word, then the prep kernel's argmax key and block counter
-  unsigned long long* key = ws.take<unsigned long long>(4);
+  // key, the threshold word, then the prep kernel's argmax key
+  unsigned long long* key = ws.take<unsigned long long>(3);
   PQI_CHECK_ARG(key);
   cudaStream_t s = as_stream(stream);
   if (!gains64) {
@@ -978,20 +974,25 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     gains64 = g;
   }
   // key (8 bytes), the shared threshold (4 bytes) and the prep kernel's
-  // argmax and counter, zeroed together
-  PQI_TRY(cudaMemsetAsync(key, 0, 32, s));
+  // argmax, zeroed together
+  PQI_TRY(cudaMemsetAsync(key, 0, 24, s));
   unsigned int* gthr = reinterpret_cast<unsigned int*>(key + 1);
   // the gains in the estimate's type (4 bytes each)
   void* gest = ws.take<float>(n);
   PQI_CHECK_ARG(gest);
+  const int pg = grid_for(n, 256, 148 * 4);
   if (w->kind == PQI_W_I8) {
-    double_prep_kernel<int8_t><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(
-        w->W_i8, w->ld, n, theta, gains64, is_spin_glass, geo, gest, key, gthr, key + 2);
+    double_prep_kernel<int8_t><<<pg, 256, 0, s>>>(gains64, n, gest, key + 2);
+    PQI_LAUNCHED("double_prep_kernel");
+    double_seed_kernel<int8_t><<<pg, 256, 0, s>>>(w->W_i8, w->ld, n, theta, gains64, is_spin_glass,
+                                                 geo, key + 2, key, gthr);
   } else {
-    double_prep_kernel<float><<<grid_for(n, 256, 148 * 4), 256, 0, s>>>(
-        w->W_f32z, w->ld, n, theta, gains64, is_spin_glass, geo, gest, key, gthr, key + 2);
+    double_prep_kernel<float><<<pg, 256, 0, s>>>(gains64, n, gest, key + 2);
+    PQI_LAUNCHED("double_prep_kernel");
+    double_seed_kernel<float><<<pg, 256, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64, is_spin_glass,
+                                                geo, key + 2, key, gthr);
   }
-  PQI_LAUNCHED("double_prep_kernel");
+  PQI_LAUNCHED("double_seed_kernel");
   // one persistent CTA per SM (the stage ring takes most of shared memory)
   static int sms = 0;
   static bool attr_set[2] = {false, false};
