@@ -524,7 +524,16 @@ def e2e_pipeline(dg, batches_host, like, G, L, steps, warmup):
     run(warmup, steps)
     end.record(comp)
     end.synchronize()
-    return start.elapsed_time(end)
+    ms = start.elapsed_time(end)
+    # the host link alone: the same copies back to back (the pipeline's floor)
+    start.record(copy)
+    with torch.cuda.stream(copy):
+        for i in range(steps):
+            dev_in[i & 1].copy_(pinned[i % nb], non_blocking=True)
+    end.record(copy)
+    end.synchronize()
+    e2e_pipeline.h2d_only_ms = start.elapsed_time(end)
+    return ms
 
 
 def plain_small_leg(reps=5):
@@ -1145,6 +1154,8 @@ def main():
             "unit": UNIT,
             "h2d_bytes_per_step": int(batches_host[0].nbytes),
             "d2h_bytes_per_step": 8,
+            "ms_per_step": e2e_ms / args.steps,
+            "h2d_only_ms_per_step": getattr(e2e_pipeline, "h2d_only_ms", float("nan")) / args.steps,
         },
         "roofline": {
             "bound": "tensor",
