@@ -388,18 +388,6 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
       : "memory");
 }
 
-// A stage's tile header, written by the producer warp before the stage's
-// copies are armed (the arrive releases it to the consumers): the tile's
-// first row (-1 ends the walk), column chunk, the rows' estimate gains and
-// bits, and the largest |row gain|.
-template <typename ET>
-struct DsTile {
-  int k0, c;
-  uint32_t xk;
-  float gt;
-  ET fk[DR];
-};
-
 template <typename WT>
 __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
     const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
@@ -413,7 +401,6 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
   extern __shared__ __align__(1024) unsigned char ring[];
   __shared__ __align__(8) uint64_t full_bar[DS_STAGES];
   __shared__ __align__(8) uint64_t empty_bar[DS_STAGES];
-  __shared__ DsTile<ET> meta[DS_STAGES];
   __shared__ uint64_t scratch[32];
   __shared__ unsigned int s_thr;
   __shared__ int s_fail;
@@ -429,57 +416,25 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
     s_fail = 0;
   }
   __syncthreads();
+  const int ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
+  const int nc = (n + CW - 1) / CW;      // column chunks
+  const int total = ng * nc;             // (n <= 46341: well inside int)
   uint64_t best = 0;
   if (warp == DS_CONSUMERS / 32) {
-    // producer: walks this CTA's tiles (a stride of gridDim.x over the
-    // rectangle of row groups x column chunks, tiles wholly at or below the
-    // diagonal skipped), writes each tile's header and arms its copies once
-    // the consumers have released the stage; a header with k0 = -1 ends
-    const int ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
-    const int nc = (n + CW - 1) / CW;      // column chunks
-    const int total = ng * nc;             // (n <= 46341: well inside int)
-    int it = 0;
-    for (int tau = blockIdx.x;; tau += gridDim.x) {
-      int rg = 0, c = 0;
-      bool end = tau >= total;
-      if (!end) {
-        rg = tau / nc;
-        c = tau - rg * nc;
+    // producer: this CTA's tiles (a stride of gridDim.x over the rectangle of
+    // row groups x column chunks, tiles wholly at or below the diagonal
+    // skipped), each into the next stage once the consumers released it
+    if (lane == 0) {
+      int it = 0;
+      for (int tau = blockIdx.x; tau < total; tau += gridDim.x) {
+        const int rg = tau / nc, c = tau - rg * nc;
         if ((c + 1) * CW <= rg * DR + 1) continue;
-      }
-      const int st = it % DS_STAGES;
-      const uint32_t use = (uint32_t)(it / DS_STAGES);
-      if (use > 0 && !tc::mbar_wait_warp(&empty_bar[st], (use - 1) & 1u)) {
-        s_fail = 1;
-        break;
-      }
-      DsTile<ET>& m = meta[st];
-      if (end) {
-        if (lane == 0) {
-          m.k0 = -1;
-          tc::mbar_arrive(&full_bar[st]);
+        const int st = it % DS_STAGES;
+        const uint32_t use = (uint32_t)(it / DS_STAGES);
+        if (use > 0 && !tc::mbar_wait(&empty_bar[st], (use - 1) & 1u)) {
+          s_fail = 1;
+          break;
         }
-        break;
-      }
-      const int k0 = rg * DR;
-      {
-        const int k = min(k0 + lane, n - 1);
-        const ET fv = lane < DR ? __ldg(gest + k) : ET(0);
-        const uint32_t bit = lane < DR ? (uint32_t)get_bit32(theta, (uint32_t)k) : 0u;
-        const uint32_t xk = __ballot_sync(0xFFFFFFFFu, bit != 0u);
-        float a = fabsf((float)fv);
-#pragma unroll
-        for (int o = 1; o < DR; o <<= 1) a = fmaxf(a, __shfl_xor_sync(0xFFFFFFFFu, a, o));
-        if (lane < DR) m.fk[lane] = fv;
-        if (lane == 0) {
-          m.k0 = k0;
-          m.c = c;
-          m.xk = xk;
-          m.gt = a;
-        }
-      }
-      __syncwarp();
-      if (lane == 0) {
         // the row segments: up to CW columns, within the padded row (ld is a
         // multiple of 128, so the size is a multiple of 512 bytes)
         const int col0 = c * CW;
@@ -488,30 +443,35 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
         unsigned char* dst = ring + (size_t)st * DS_TILE_BYTES;
 #pragma unroll
         for (int i = 0; i < DR; ++i) {
-          const int k = min(k0 + i, n - 1);
+          const int k = min(rg * DR + i, n - 1);
           bulk_copy_g2s(dst + i * DS_ROW_BYTES, Wp + (size_t)k * ld + col0, bytes, &full_bar[st]);
         }
+        ++it;
       }
-      ++it;
     }
   } else {
+    // consumers: the same tiles in the same order; each tile's row gains and
+    // bits, this thread's column gains and bits and the threshold are loaded
+    // while the tile's copies land
     float thr = -INFINITY;
-    for (int it = 0;; ++it) {
+    int it = 0;
+    for (int tau = blockIdx.x; tau < total; tau += gridDim.x) {
+      const int rg = tau / nc, c = tau - rg * nc;
+      if ((c + 1) * CW <= rg * DR + 1) continue;
       const int st = it % DS_STAGES;
       const uint32_t use = (uint32_t)(it / DS_STAGES);
-      thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(gthr))));
-      if (!tc::mbar_wait_warp(&full_bar[st], use & 1u)) {
-        s_fail = 1;
-        break;
-      }
-      const DsTile<ET>& m = meta[st];
-      const int k0 = m.k0;
-      if (k0 < 0) break;
-      const int c = m.c;
-      const uint32_t xk = m.xk;
+      ++it;
+      const int k0 = rg * DR;
       ET fk[DR];
+      uint32_t xk = 0;
+      float gt = 0.0f;
 #pragma unroll
-      for (int i = 0; i < DR; ++i) fk[i] = m.fk[i];
+      for (int i = 0; i < DR; ++i) {
+        const int k = min(k0 + i, n - 1);
+        fk[i] = __ldg(gest + k);
+        if constexpr (!INT) gt = fmaxf(gt, fabsf(fk[i]));
+        xk |= (uint32_t)get_bit32(theta, (uint32_t)k) << i;
+      }
       const int l0 = c * CW + (int)threadIdx.x * VEC;
       ET fl[VEC];
       float flmax = 0.0f;
@@ -522,6 +482,11 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
         fl[e] = l < n ? __ldg(gest + l) : ET(0);
         if constexpr (!INT) flmax = fmaxf(flmax, fabsf(fl[e]));
       }
+      thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(gthr))));
+      if (!tc::mbar_wait_warp(&full_bar[st], use & 1u)) {
+        s_fail = 1;
+        break;
+      }
       const unsigned char* tile = ring + (size_t)st * DS_TILE_BYTES + threadIdx.x * 16;
       WT w[DR][VEC];
 #pragma unroll
@@ -529,7 +494,7 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
         const int4 v = *reinterpret_cast<const int4*>(tile + i * DS_ROW_BYTES);
         memcpy(&w[i][0], &v, 16);
       }
-      const float base = m.gt + flmax;
+      const float base = gt + flmax;
       float cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
       int cut_i = thr > -INFINITY ? (int)thr : INT_MIN;
       // (columns past the copied row segment hold stale bytes: such a thread
