@@ -392,7 +392,8 @@ template <typename WT>
 __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
     const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
     const double* __restrict__ g64, const void* __restrict__ gest_v, int spin, SelGeom geo,
-    unsigned long long* key, unsigned int* gthr) {
+    unsigned long long* key, unsigned int* gthr, unsigned int* done, float* best_val,
+    int* best_idx) {
   constexpr int VEC = 16 / (int)sizeof(WT);  // columns per consumer thread
   constexpr int CW = VEC * DS_CONSUMERS;    // columns per tile (DS_ROW_BYTES of a row)
   constexpr bool INT = sizeof(WT) == 1;
@@ -435,16 +436,19 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
           s_fail = 1;
           break;
         }
-        // the row segments: up to CW columns, within the padded row (ld is a
-        // multiple of 128, so the size is a multiple of 512 bytes)
+        // the row segments from the first column above the tile's first row
+        // (rounded down to 16 bytes) to the chunk's end, within the padded
+        // row (ld is a multiple of 128); column l sits at (l - col0) of its
+        // row's slot either way
         const int col0 = c * CW;
-        const uint32_t bytes = (uint32_t)(min(CW, ld - col0) * (int)sizeof(WT));
+        const int cs = max(col0, (rg * DR + 1) & ~(16 / (int)sizeof(WT) - 1));
+        const uint32_t bytes = (uint32_t)((min(col0 + CW, ld) - cs) * (int)sizeof(WT));
         tc::mbar_expect_tx(&full_bar[st], bytes * DR);
-        unsigned char* dst = ring + (size_t)st * DS_TILE_BYTES;
+        unsigned char* dst = ring + (size_t)st * DS_TILE_BYTES + (size_t)(cs - col0) * sizeof(WT);
 #pragma unroll
         for (int i = 0; i < DR; ++i) {
           const int k = min(rg * DR + i, n - 1);
-          bulk_copy_g2s(dst + i * DS_ROW_BYTES, Wp + (size_t)k * ld + col0, bytes, &full_bar[st]);
+          bulk_copy_g2s(dst + i * DS_ROW_BYTES, Wp + (size_t)k * ld + cs, bytes, &full_bar[st]);
         }
         ++it;
       }
@@ -537,7 +541,9 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
         for (int i = 1; i < DR; ++i) amax = fmaxf(amax, ra[i]);
         any = amax >= cut;
       }
-      if (any && l0 < n) {
+      // (columns before the copied part hold stale bytes: every pair there
+      // has l <= k, and a thread with no column after the copy start has none)
+      if (any && l0 < n && l0 + VEC > max(c * CW, (k0 + 1) & ~(VEC - 1))) {
         const WT* tw = reinterpret_cast<const WT*>(ring + (size_t)st * DS_TILE_BYTES);
         // float: only the rows whose largest estimate reaches the cut
         uint32_t rows = (1u << DR) - 1u;
@@ -593,8 +599,20 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
     }
   }
   best = block_max_u64(best, scratch);
-  // a wait that ran out leaves no result (key 0: value -inf, index -1)
-  if (threadIdx.x == 0 && best && !s_fail) atomicMax(key, (unsigned long long)best);
+  // a wait that ran out leaves no result (key 0: value -inf, index -1); the
+  // last CTA to finish decodes the selection
+  if (threadIdx.x == 0) {
+    if (best && !s_fail) atomicMax(key, (unsigned long long)best);
+    __threadfence();
+    if (atomicAdd(done, 1u) == gridDim.x - 1) {
+      __threadfence();
+      float v;
+      int64_t i;
+      sel_decode(*(volatile unsigned long long*)key, geo, &v, &i);
+      if (best_val) *best_val = v;
+      if (best_idx) *best_idx = (int)i;
+    }
+  }
 }
 
 // Apply one or two flips to (theta, gains64). x = 2s - 1 of the state before.
@@ -927,8 +945,8 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
   SelGeom geo;
   PQI_CHECK_ARG(make_sel_geom(combo, global_size, local_size, &geo));
   Workspace ws(workspace, workspace_bytes);
-  // key, the threshold word, then the prep kernel's argmax key
-  unsigned long long* key = ws.take<unsigned long long>(3);
+  // key, the threshold word, the prep kernel's argmax key, the CTA counter
+  unsigned long long* key = ws.take<unsigned long long>(4);
   PQI_CHECK_ARG(key);
   cudaStream_t s = as_stream(stream);
   if (!gains64) {
@@ -938,9 +956,9 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     if (rc) return rc;
     gains64 = g;
   }
-  // key (8 bytes), the shared threshold (4 bytes) and the prep kernel's
-  // argmax, zeroed together
-  PQI_TRY(cudaMemsetAsync(key, 0, 24, s));
+  // key (8 bytes), the shared threshold (4 bytes), the prep kernel's argmax
+  // and the stream kernel's CTA counter, zeroed together
+  PQI_TRY(cudaMemsetAsync(key, 0, 32, s));
   unsigned int* gthr = reinterpret_cast<unsigned int*>(key + 1);
   // the gains in the estimate's type (4 bytes each)
   void* gest = ws.take<float>(n);
@@ -973,15 +991,15 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     attr_set[i8] = true;
   }
   if (i8) {
-    double_stream_kernel<int8_t><<<sms, DS_THREADS, DS_SMEM, s>>>(w->W_i8, w->ld, n, theta, gains64, gest,
-                                                                  is_spin_glass, geo, key, gthr);
+    double_stream_kernel<int8_t><<<sms, DS_THREADS, DS_SMEM, s>>>(
+        w->W_i8, w->ld, n, theta, gains64, gest, is_spin_glass, geo, key, gthr,
+        reinterpret_cast<unsigned int*>(key + 3), best_energy, best_index);
   } else {
-    double_stream_kernel<float><<<sms, DS_THREADS, DS_SMEM, s>>>(w->W_f32z, w->ld, n, theta, gains64, gest,
-                                                                 is_spin_glass, geo, key, gthr);
+    double_stream_kernel<float><<<sms, DS_THREADS, DS_SMEM, s>>>(
+        w->W_f32z, w->ld, n, theta, gains64, gest, is_spin_glass, geo, key, gthr,
+        reinterpret_cast<unsigned int*>(key + 3), best_energy, best_index);
   }
   PQI_LAUNCHED("double_stream_kernel");
-  select_finish_kernel<<<1, 1, 0, s>>>(key, geo, best_energy, best_index);
-  PQI_LAUNCHED("select_finish_kernel");
   return PQI_OK;
 }
 
