@@ -678,7 +678,7 @@ def flip_bandwidth_leg(n=8192, tasks=1776, fields="auto"):
     _, e64 = dg.rescore(b2[pick].contiguous(), rows=len(pick))
     tracked = v2[pick]
     rel = float(((tracked - e64).abs() / e64.abs().clamp_min(1e-300)).max().item())
-    used = fields if fields != "auto" else ("f32" if n > 4096 else "f64")
+    used = fields if fields != "auto" else ("f32" if n > 24576 else "f64")
     return {
         "workload": f"SK n={n} float32, {tasks} starts of the batched ascent, 2048 flips each after the starting fields (timed apart and subtracted), {used} local fields, float64 acceptance and running value",
         "tracked_value_rel_err_vs_fp64": rel,
@@ -1191,7 +1191,7 @@ def main():
             line["batched"] = batched_leg()
             line["learned"] = learned_leg()
             line["flip_updates"] = flip_bandwidth_leg()
-            line["flip_updates_f64_fields"] = flip_bandwidth_leg(fields="f64")
+            line["flip_updates_f32_fields"] = flip_bandwidth_leg(fields="f32")
         if world == 1:
             try:
                 line["cpu_baseline"] = cpu_baseline(W, make_batch(0, 2048))

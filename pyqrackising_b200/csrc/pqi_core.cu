@@ -517,22 +517,28 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
           }
         }
       } else {
-        // the largest estimate of the thread's pairs, f_k + (f_l + 2 (-/+ W)):
-        // W's sign bit flipped by a row mask and a column mask (one three-way
-        // XOR), one FMA and one max per pair. (The grouping differs from the
-        // exact path's (f_k + f_l) + 2 (-/+ W) by a few units in the last
-        // place, far inside the cut's 2^-20 margin.)
-        uint32_t cm[VEC];
+        // the largest estimate of the thread's pairs, f_k + (f_l -/+ 2 W).
+        // (The grouping differs from the exact path's (f_k + f_l) -/+ 2 W by
+        // a few units in the last place, far inside the cut's 2^-20 margin.)
+        // the coefficient of W_kl is -2 where the bits agree, else +2: for a
+        // row with bit 1 that is cp[e] (from column l's bit), for a row with
+        // bit 0 its negation. The rows' bits are the same for every thread,
+        // so the branch on them is uniform and each pair costs one FMA and
+        // one max.
+        float cp[VEC];
 #pragma unroll
-        for (int e = 0; e < VEC; ++e) cm[e] = ((lw >> e) & 1u) << 31;
+        for (int e = 0; e < VEC; ++e) cp[e] = ((lw >> e) & 1u) ? -2.0f : 2.0f;
 #pragma unroll
         for (int i = 0; i < DR; ++i) {
-          const uint32_t rm = (((xk >> i) & 1u) ^ 1u) << 31;
-          float r = -INFINITY;
+          float r;
+          if ((xk >> i) & 1u) {
+            r = fmaf(cp[0], w[i][0], fl[0]);
 #pragma unroll
-          for (int e = 0; e < VEC; ++e) {
-            const float cw = __uint_as_float(__float_as_uint(w[i][e]) ^ rm ^ cm[e]);
-            r = fmaxf(r, fmaf(2.0f, cw, fl[e]));
+            for (int e = 1; e < VEC; ++e) r = fmaxf(r, fmaf(cp[e], w[i][e], fl[e]));
+          } else {
+            r = fmaf(-cp[0], w[i][0], fl[0]);
+#pragma unroll
+            for (int e = 1; e < VEC; ++e) r = fmaxf(r, fmaf(-cp[e], w[i][e], fl[e]));
           }
           ra[i] = fk[i] + r;
         }
