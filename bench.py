@@ -362,8 +362,10 @@ def time_to_best_learned(n=8192, starts=32, cluster=8, rounds=4, kick=64, temper
          kick distributions by pqi_mpnn_kick_cdf);
       3. `rounds` of the batched iterated search from those optima with
          learned kicks.
-    time_to_plain_best is the elapsed time at the end of the first stage whose
-    running best reaches the plain form's best (None if none does). Beside
+    time_to_plain_best is the first stage run again in target mode (every
+    start stops once one holds the plain form's best; a device flag), or else
+    the end of the first stage whose running best reaches it (None if none
+    does). Beside
     stage 3, the same search with uniform kicks from the same optima, seeds
     and budget: what the network adds over the method without it."""
     import importlib
@@ -420,7 +422,15 @@ def time_to_best_learned(n=8192, starts=32, cluster=8, rounds=4, kick=64, temper
     t_uniform = time.perf_counter() - ta
     best = int(torch.argmax(vP).item())
     _, e64 = dg.rescore(wP[best].contiguous())
-    ttb = t1 if reached(b1) else (t3 if reached(max(b1, b3)) else None)
+    # the first stage in target mode: every start stops once one holds the
+    # plain form's best (the later stages start from full ascents above)
+    bs.cluster_ascent(tasks, w0, True, cluster_size=cluster, target=e_plain)  # warm
+    torch.cuda.synchronize()
+    tt = time.perf_counter()
+    vT, wT, _, _ = bs.cluster_ascent(tasks, w0, True, cluster_size=cluster, target=e_plain)
+    bT = float(vT.max().item())
+    t_target = time.perf_counter() - tt
+    ttb = t_target if reached(bT) else (t1 if reached(b1) else (t3 if reached(max(b1, b3)) else None))
     return {
         "workload": f"SK n={n}, J~N(0,1)/sqrt(n) float32, is_spin_glass; plain: local-search loop from 1 start; "
                     f"batched + learned: {starts} starts, cluster ascent ({cluster} CTAs per start), the trained "
@@ -435,7 +445,9 @@ def time_to_best_learned(n=8192, starts=32, cluster=8, rounds=4, kick=64, temper
         "learned_minus_uniform": b3 - bU,
         "best_energy_rel_err_vs_fp64": abs(b3 - float(e64.item())) / max(abs(float(e64.item())), 1e-300),
         "status": int(sP.item()),
+        "stage_ascent_to_target_s": t_target, "stage_ascent_to_target_best": bT,
         "time_to_plain_best_s": ttb,
+        "time_to_plain_best_basis": "the first stage in target mode (the learned stages come after the plain best is reached)",
         "speedup": (t_plain / ttb) if ttb else None,
     }
 
