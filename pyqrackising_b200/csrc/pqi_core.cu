@@ -302,6 +302,15 @@ __device__ __forceinline__ uint64_t pair_key(float v, uint32_t t, uint32_t j, co
   return ((uint64_t)ord_f32(v) << 32) | (uint64_t)(0xFFFFFFFFu - ((grp * geo.L + r) * geo.J + j));
 }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may start once every CTA of the kernel before it has called
+// launch_dependents; wait() then blocks until that kernel has completed and
+// its writes are visible (a no-op without such a predecessor).
+__device__ __forceinline__ void pdl_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Before the pass: the gains in the estimate's type (float32 for float
 // weights, int32 - exact - for int8 weights) and the node m of the largest
 // gain (ctl[0]: ordered gain << 32 | ~node, so the lowest node on ties).
@@ -311,6 +320,7 @@ __global__ void __launch_bounds__(256) double_prep_kernel(const double* __restri
                                                           unsigned long long* ctl) {
   constexpr bool INT = sizeof(WT) == 1;
   __shared__ uint64_t scratch[32];
+  pdl_launch_dependents();  // the seed kernel may start (it waits for this one)
   uint64_t am = 0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
     const double gk = g64[k];
@@ -336,6 +346,8 @@ __global__ void __launch_bounds__(256) double_seed_kernel(
     const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
     const double* __restrict__ g64, int spin, SelGeom geo, const unsigned long long* ctl,
     unsigned long long* key, unsigned int* gthr) {
+  pdl_launch_dependents();  // the pass may start streaming W
+  pdl_wait();               // the prep kernel's gains and argmax
   const uint64_t top = *ctl;
   if (!top) return;
   const int m = (int)(0xFFFFFFFFu - (uint32_t)top);
@@ -456,7 +468,9 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
   } else {
     // consumers: the same tiles in the same order; each tile's row gains and
     // bits, this thread's column gains and bits and the threshold are loaded
-    // while the tile's copies land
+    // while the tile's copies land. The gains and the seeded threshold come
+    // from the kernels before this one: wait for them (the producer does not)
+    pdl_wait();
     float thr = -INFINITY;
     int it = 0;
     for (int tau = blockIdx.x; tau < total; tau += gridDim.x) {
@@ -970,16 +984,30 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
   void* gest = ws.take<float>(n);
   PQI_CHECK_ARG(gest);
   const int pg = grid_for(n, 256, 148 * 4);
+  // the seed kernel and the pass are launched as programmatic dependents: the
+  // pass's producer streams W while the gains are converted and the
+  // threshold seeded; its consumers wait for both (pdl_wait)
+  cudaLaunchAttribute pdl[1];
+  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  pdl[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t seed_cfg = {};
+  seed_cfg.gridDim = dim3(pg);
+  seed_cfg.blockDim = dim3(256);
+  seed_cfg.stream = s;
+  seed_cfg.attrs = pdl;
+  seed_cfg.numAttrs = 1;
   if (w->kind == PQI_W_I8) {
     double_prep_kernel<int8_t><<<pg, 256, 0, s>>>(gains64, n, gest, key + 2);
     PQI_LAUNCHED("double_prep_kernel");
-    double_seed_kernel<int8_t><<<pg, 256, 0, s>>>(w->W_i8, w->ld, n, theta, gains64, is_spin_glass,
-                                                 geo, key + 2, key, gthr);
+    PQI_TRY(cudaLaunchKernelEx(&seed_cfg, double_seed_kernel<int8_t>, (const int8_t*)w->W_i8, w->ld, n,
+                               theta, gains64, is_spin_glass, geo, (const unsigned long long*)(key + 2),
+                               key, gthr));
   } else {
     double_prep_kernel<float><<<pg, 256, 0, s>>>(gains64, n, gest, key + 2);
     PQI_LAUNCHED("double_prep_kernel");
-    double_seed_kernel<float><<<pg, 256, 0, s>>>(w->W_f32z, w->ld, n, theta, gains64, is_spin_glass,
-                                                geo, key + 2, key, gthr);
+    PQI_TRY(cudaLaunchKernelEx(&seed_cfg, double_seed_kernel<float>, (const float*)w->W_f32z, w->ld, n,
+                               theta, gains64, is_spin_glass, geo, (const unsigned long long*)(key + 2),
+                               key, gthr));
   }
   PQI_LAUNCHED("double_seed_kernel");
   // one persistent CTA per SM (the stage ring takes most of shared memory)
@@ -996,14 +1024,22 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     PQI_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, DS_SMEM));
     attr_set[i8] = true;
   }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(sms);
+  cfg.blockDim = dim3(DS_THREADS);
+  cfg.dynamicSmemBytes = DS_SMEM;
+  cfg.stream = s;
+  cfg.attrs = pdl;
+  cfg.numAttrs = 1;
+  unsigned int* done = reinterpret_cast<unsigned int*>(key + 3);
   if (i8) {
-    double_stream_kernel<int8_t><<<sms, DS_THREADS, DS_SMEM, s>>>(
-        w->W_i8, w->ld, n, theta, gains64, gest, is_spin_glass, geo, key, gthr,
-        reinterpret_cast<unsigned int*>(key + 3), best_energy, best_index);
+    PQI_TRY(cudaLaunchKernelEx(&cfg, double_stream_kernel<int8_t>, (const int8_t*)w->W_i8, w->ld, n,
+                               theta, gains64, (const void*)gest, is_spin_glass, geo, key, gthr, done,
+                               best_energy, best_index));
   } else {
-    double_stream_kernel<float><<<sms, DS_THREADS, DS_SMEM, s>>>(
-        w->W_f32z, w->ld, n, theta, gains64, gest, is_spin_glass, geo, key, gthr,
-        reinterpret_cast<unsigned int*>(key + 3), best_energy, best_index);
+    PQI_TRY(cudaLaunchKernelEx(&cfg, double_stream_kernel<float>, (const float*)w->W_f32z, w->ld, n,
+                               theta, gains64, (const void*)gest, is_spin_glass, geo, key, gthr, done,
+                               best_energy, best_index));
   }
   PQI_LAUNCHED("double_stream_kernel");
   return PQI_OK;
