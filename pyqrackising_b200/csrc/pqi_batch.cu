@@ -203,13 +203,6 @@ __device__ __forceinline__ void flip_and_select(const TaskCtx<WT, GT>& c, int k,
     }
   };
   constexpr int PER = STG ? CH + kStageGroups : CH;  // groups per pass
-  // a row longer than one pass: the later passes' 16-byte pieces are asked
-  // into L2 now, so their loads wait on L2 rather than DRAM (one prefetch per
-  // 128-byte line)
-  if (!STG && k >= 0 && (threadIdx.x & 7) == 0) {
-    for (int v = 4 * threadIdx.x + PER * stride; v < n; v += stride)
-      asm volatile("prefetch.global.L2 [%0];" ::"l"(row + v));
-  }
   for (int base = 4 * threadIdx.x; base < n; base += PER * stride) {
     if constexpr (STG) {
       // the pass's last kStageGroups groups go to shared memory first, so the
