@@ -1191,13 +1191,15 @@ def main():
             "ops_note": "int8 multiply-adds counted as 2 ops (TOPS)",
             # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this
             # workload (profiles/score_tc_kernel_er2048_b65536.md)
-            "traffic": 195.9e6,
+            "traffic": 196.3e6,
             "traffic_unit": "bytes per launch (ncu)",
             "algorithmic_bytes_per_launch": float(BATCH * N_NODES + N_NODES * N_NODES + BATCH * N_NODES // 8),
             "peak_basis": f"int8 dense = 2 x bf16 dense ({src} bf16 {bf16} TFLOP/s)",
             "kernel": "score_tc_kernel<int8> (tcgen05 GEMM + row-dot epilogue), CUDA events around the launch",
             "kernel_ms": kernel_ms,
             "algorithmic_ops_per_launch": ops,
+            # the whole step (expansion pass, GEMM, selection) against the same peak
+            "frac_step": ops / (ms_per_step / 1000.0) / 1e12 / int8_peak,
         },
         # per step: score_tc_kernel (the L2 flush is torch's fill)
         "gpu_launches": args.steps,
