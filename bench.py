@@ -466,7 +466,7 @@ def time_to_best_learned(n=8192, starts=32, cluster=8, rounds=4, kick=64, temper
 
 
 def scoring_batch_leg(dg, batch=4096, reps=50):
-    """The scoring kernel at config 2's own parallel seed count (4096
+    """The scoring kernel at the parallel seed count of the ER-2048 solve (4096
     candidates, a GEMM 16x smaller than the headline's): device time per call
     (CUDA events around the GEMM launch and around the whole call), the
     fraction of the int8 peak, L2 flushed before each call."""
@@ -501,7 +501,7 @@ def scoring_batch_leg(dg, batch=4096, reps=50):
     km = float(np.median(k_ms))
     ops = 2.0 * batch * N_NODES * N_NODES
     return {
-        "workload": f"ER G(n=2048,p=0.5) unit weights, {batch} candidates per call (config 2's parallel seeds)",
+        "workload": f"ER G(n=2048,p=0.5) unit weights, {batch} candidates per call (the solve's parallel seeds)",
         "kernel_ms": km,
         "call_ms": float(np.median(s_ms)),
         "candidates_per_s": batch / (float(np.median(s_ms)) / 1e3),
