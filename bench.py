@@ -1202,7 +1202,9 @@ def main():
             "frac_step": ops / (ms_per_step / 1000.0) / 1e12 / int8_peak,
         },
         # per step: score_tc_kernel (the L2 flush is torch's fill)
-        "gpu_launches": args.steps,
+        # per step the library launches the +-1 expansion and the scoring GEMM
+        # (the zeroing of its selection words is a memset, not a kernel)
+        "gpu_launches": 2 * args.steps,
         "best_over_ranks": {"value": best_value, "rank": best_rank},
         "wall_s_timed_loop": wall,
     }
