@@ -274,8 +274,8 @@ __global__ void select_finish_kernel(const unsigned long long* key, SelGeom geo,
 // is float(d) (x2 for a spin glass) and its selection is the maximum 64-bit
 // key (sel_key) over all pairs k < l in k-major order.
 //
-// The upper triangle is cut into tiles of DR rows x CW columns (CW = 2048
-// float32 or 8192 int8 columns: 8 KB of each row), each W element read once.
+// The upper triangle is cut into tiles of 16 rows x 1024 float32 columns
+// (8 rows x 4096 int8 columns: 4 KB of each row), each W element read once.
 // Every pair first gets an fp32 estimate a = f_k + f_l + c W_kl (f = the gain
 // in the estimate's type, c = -2 when the bits agree, else +2). |a - value|
 // is below 2^-22 (|g_k| + |g_l| + |a|), so a pair with a < thr - delta,
@@ -286,7 +286,7 @@ __global__ void select_finish_kernel(const unsigned long long* key, SelGeom geo,
 // block (shared memory) and across blocks (one global word), both as
 // order-preserving uint32 under atomicMax, and seeded before the pass.
 
-constexpr int DR = 8;  // rows per tile
+constexpr int DS_ROWS = 16;  // rows per tile (float32 weights)
 
 __device__ __forceinline__ float thr_of(uint32_t o) {
   // ordered 0 (nothing published yet) and anything below -inf read as -inf
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(256) double_seed_kernel(
 }
 
 // The same pass with W streamed through shared memory: one persistent CTA per
-// SM, a producer warp copying each tile's DR row segments of DS_ROW_BYTES
+// SM, a producer warp copying each tile's row segments of DS_ROW_BYTES
 // (cp.async.bulk, completion counted on the stage's mbarrier) into a ring of
 // DS_STAGES stages, and DS_CONSUMERS threads that score the tile from shared
 // memory (the estimate pass, then the exact path for flagged tiles) and
@@ -385,10 +385,10 @@ __global__ void __launch_bounds__(256) double_seed_kernel(
 // DS_STAGES tiles ahead of the scoring, so HBM sees a deep queue of large
 // requests whatever the scoring's latency.
 constexpr int DS_STAGES = 3;
-constexpr int DS_CONSUMERS = 512;
+constexpr int DS_CONSUMERS = 256;
 constexpr int DS_THREADS = DS_CONSUMERS + 32;
-constexpr int DS_ROW_BYTES = 16 * DS_CONSUMERS;  // 8 KB of a row per tile
-constexpr int DS_TILE_BYTES = DR * DS_ROW_BYTES;
+constexpr int DS_ROW_BYTES = 16 * DS_CONSUMERS;  // 4 KB of a row per tile
+constexpr int DS_TILE_BYTES = DS_ROWS * DS_ROW_BYTES;
 constexpr int DS_SMEM = DS_STAGES * DS_TILE_BYTES;
 
 __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
@@ -409,6 +409,9 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
   constexpr int VEC = 16 / (int)sizeof(WT);  // columns per consumer thread
   constexpr int CW = VEC * DS_CONSUMERS;    // columns per tile (DS_ROW_BYTES of a row)
   constexpr bool INT = sizeof(WT) == 1;
+  // rows per tile: 16 for float32 (64 KB stages), 8 for int8 (its graphs are
+  // small and L2-resident: more, smaller tiles keep every SM busy)
+  constexpr int DR = INT ? 8 : DS_ROWS;
   typedef typename std::conditional<INT, int, float>::type ET;
   const ET* __restrict__ gest = static_cast<const ET*>(gest_v);
   extern __shared__ __align__(1024) unsigned char ring[];
