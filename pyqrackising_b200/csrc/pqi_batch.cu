@@ -357,15 +357,24 @@ __global__ void __launch_bounds__(256) start_fields_kernel(
       uint32_t xw[4];
 #pragma unroll
       for (int j = 0; j < 4; ++j) xw[j] = Xs[4 * ty + j];
+      // acc += (+-1) w as one fused multiply-add with an exact product: the
+      // same rounding as the add of +-w, and the sign is chosen once per task
+      // and row instead of once per element
       auto row = [&](int r) {
         AT w[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) w[i] = Ws[r][4 * tx + i];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          const bool bit = (xw[j] >> r) & 1u;
+          const AT sj = ((xw[j] >> r) & 1u) ? (AT)1 : (AT)-1;
 #pragma unroll
-          for (int i = 0; i < 4; ++i) acc[i][j] += bit ? w[i] : -w[i];
+          for (int i = 0; i < 4; ++i) {
+            if constexpr (std::is_same<AT, double>::value) {
+              acc[i][j] = fma(sj, w[i], acc[i][j]);
+            } else {
+              acc[i][j] += sj * w[i];
+            }
+          }
         }
       };
       if (n - u0 >= SF_U) {
