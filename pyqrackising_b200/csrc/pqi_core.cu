@@ -284,7 +284,8 @@ __global__ void select_finish_kernel(const unsigned long long* key, SelGeom geo,
 // maximum and is skipped. Only tiles holding a pair at the cut - the rare
 // near-maxima - take pairs' exact float64 values and keys. thr is shared per
 // block (shared memory) and across blocks (one global word), both as
-// order-preserving uint32 under atomicMax, and seeded before the pass.
+// order-preserving uint32 under atomicMax, and seeded in every block from the
+// pairs of the node with the largest gain.
 
 constexpr int DS_ROWS = 16;  // rows per tile (float32 weights)
 
@@ -312,57 +313,88 @@ __device__ __forceinline__ void pdl_launch_dependents() {
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // Before the pass: the gains in the estimate's type (float32 for float
-// weights, int32 - exact - for int8 weights) and the node m of the largest
-// gain (ctl[0]: ordered gain << 32 | ~node, so the lowest node on ties).
+// weights, int32 - exact - for int8 weights), zero from n up to npad (the pass
+// reads them as whole vectors), and per CTA two partials: the node of the
+// largest gain (ordered gain << 32 | ~node, so the lowest node on ties) and the
+// largest |gain| (ordered float32). CTA 0 also clears the pass's result key,
+// shared threshold and CTA counter (ctl[0], ctl[1], ctl[3]): the pass touches
+// them only after this kernel has completed.
 template <typename WT>
 __global__ void __launch_bounds__(256) double_prep_kernel(const double* __restrict__ g64, int n,
-                                                          void* __restrict__ gest_v,
+                                                          int npad, void* __restrict__ gest_v,
+                                                          unsigned long long* __restrict__ parts,
                                                           unsigned long long* ctl) {
   constexpr bool INT = sizeof(WT) == 1;
   __shared__ uint64_t scratch[32];
-  pdl_launch_dependents();  // the seed kernel may start (it waits for this one)
-  uint64_t am = 0;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const double gk = g64[k];
-    if constexpr (INT) {
-      static_cast<int*>(gest_v)[k] = (int)llrint(gk);
+  pdl_launch_dependents();  // the pass may start streaming W
+  uint64_t am = 0, ga = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < npad; k += gridDim.x * blockDim.x) {
+    if (k < n) {
+      const double gk = g64[k];
+      const float fk = (float)gk;
+      if constexpr (INT) {
+        static_cast<int*>(gest_v)[k] = (int)llrint(gk);
+      } else {
+        static_cast<float*>(gest_v)[k] = fk;
+      }
+      const uint64_t a = ((uint64_t)ord_f32(fk) << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)k);
+      am = a > am ? a : am;
+      if (fk == fk) ga = max(ga, (uint64_t)ord_f32(fabsf(fk)));
+    } else if constexpr (INT) {
+      static_cast<int*>(gest_v)[k] = 0;
     } else {
-      static_cast<float*>(gest_v)[k] = (float)gk;
+      static_cast<float*>(gest_v)[k] = 0.0f;
     }
-    const uint64_t a = ((uint64_t)ord_f32((float)gk) << 32) | (uint64_t)(0xFFFFFFFFu - (uint32_t)k);
-    am = a > am ? a : am;
   }
   am = block_max_u64(am, scratch);
-  if (threadIdx.x == 0 && am) atomicMax(ctl, (unsigned long long)am);
+  ga = block_max_u64(ga, scratch);
+  if (threadIdx.x == 0) {
+    parts[blockIdx.x] = am;
+    parts[gridDim.x + blockIdx.x] = ga;
+    if (blockIdx.x == 0) {
+      ctl[0] = 0ull;
+      ctl[1] = 0ull;
+      ctl[3] = 0ull;
+    }
+  }
 }
 
 // A first threshold close to the maximum: every pair (k, m) with the node m
-// of the largest gain taken exactly - the best pairs usually contain the
-// best single node, so few tiles then hold a pair at the cut. Their keys go
-// into the result, the largest selectable value into the shared threshold
-// (one atomic per warp).
+// of the largest gain taken exactly - the best pairs usually contain the best
+// single node, so few tiles then hold a pair at the cut. Every CTA folds the
+// prep kernel's partials into m; W is symmetric, so W_km is read from row m.
+// The pairs' keys go into the result, the largest selectable value into the
+// shared threshold (one atomic per warp).
 template <typename WT>
 __global__ void __launch_bounds__(256) double_seed_kernel(
     const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
-    const double* __restrict__ g64, int spin, SelGeom geo, const unsigned long long* ctl,
-    unsigned long long* key, unsigned int* gthr) {
+    const double* __restrict__ g64, int spin, SelGeom geo,
+    const unsigned long long* __restrict__ parts, int nparts, unsigned long long* key,
+    unsigned int* gthr) {
+  __shared__ uint64_t scratch[32];
   pdl_launch_dependents();  // the pass may start streaming W
-  pdl_wait();               // the prep kernel's gains and argmax
-  const uint64_t top = *ctl;
-  if (!top) return;
-  const int m = (int)(0xFFFFFFFFu - (uint32_t)top);
+  pdl_wait();               // the prep kernel's partials and cleared words
+  uint64_t am = 0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    const uint64_t a = parts[i];
+    am = a > am ? a : am;
+  }
+  am = block_max_u64(am, scratch);
+  const int m = (int)(0xFFFFFFFFu - (uint32_t)am);
   const uint32_t xm = (uint32_t)get_bit32(theta, (uint32_t)m);
+  const double gm = g64[m];
+  const WT* __restrict__ rowm = Wp + (size_t)m * ld;
   for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
     const int k = base + (int)threadIdx.x;
     uint64_t kk = 0;
     unsigned int o = 0;
     if (k < n && k != m) {
-      const int a = min(k, m), b = max(k, m);
-      const double wd = (double)Wp[(size_t)a * ld + b];
+      const double wd = (double)rowm[k];
       const bool agree = (uint32_t)get_bit32(theta, (uint32_t)k) == xm;
-      float v = (float)(g64[a] + g64[b] - (agree ? 2.0 * wd : -2.0 * wd));
+      float v = (float)(g64[k] + gm - (agree ? 2.0 * wd : -2.0 * wd));
       const float vu = v;
       if (spin) v *= 2.0f;
+      const int a = min(k, m), b = max(k, m);
       const uint32_t c = (uint32_t)(pair_base(a, n) + (long long)(b - a - 1));
       kk = pair_key(v, c % geo.G, c / geo.G, geo);
       if (kk != 0ull) o = ord_f32(vu);
@@ -376,20 +408,23 @@ __global__ void __launch_bounds__(256) double_seed_kernel(
   }
 }
 
-// The same pass with W streamed through shared memory: one persistent CTA per
-// SM, a producer warp copying each tile's row segments of DS_ROW_BYTES
+// The pass streams W through shared memory: one persistent CTA per SM, a
+// producer warp copying each tile's row segments of DS_ROW_BYTES
 // (cp.async.bulk, completion counted on the stage's mbarrier) into a ring of
 // DS_STAGES stages, and DS_CONSUMERS threads that score the tile from shared
-// memory (the estimate pass, then the exact path for flagged tiles) and
-// release the stage. The copies run up to
-// DS_STAGES tiles ahead of the scoring, so HBM sees a deep queue of large
-// requests whatever the scoring's latency.
+// memory (the estimate, then the exact path for the rare flagged rows) and
+// release the stage. The copies run up to DS_STAGES tiles ahead of the
+// scoring, so HBM sees a deep queue of large requests whatever the scoring's
+// latency.
 constexpr int DS_STAGES = 3;
 constexpr int DS_CONSUMERS = 256;
 constexpr int DS_THREADS = DS_CONSUMERS + 32;
 constexpr int DS_ROW_BYTES = 16 * DS_CONSUMERS;  // 4 KB of a row per tile
 constexpr int DS_TILE_BYTES = DS_ROWS * DS_ROW_BYTES;
 constexpr int DS_SMEM = DS_STAGES * DS_TILE_BYTES;
+// the gains in the estimate's type are padded to a multiple of this many
+// entries (a whole tile's columns for either weight type)
+constexpr int DS_GEST_PAD = 4096;
 
 __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
                                               uint64_t* bar) {
@@ -400,10 +435,67 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32
       : "memory");
 }
 
+// Packed float32 pairs: d = a * b + c per half, round to nearest (the same
+// rounding as fmaf on each half).
+__device__ __forceinline__ uint64_t pack2(float lo, float hi) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void unpack2(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+
+// The pass's tiles: the rectangle of row groups x column chunks in row group
+// major order, every CTA taking tiles b, b + gridDim.x, ... and skipping those
+// wholly at or below the diagonal ((c + 1) CW <= rg DR + 1). The producer and
+// the consumers walk the same sequence; a step is a few adds (the stride's
+// quotient and remainder by the chunk count are taken once).
+template <int CW, int DR>
+struct TileWalk {
+  int ng, nc, rg, c, sq, sr;
+  __device__ __forceinline__ TileWalk(int n, int first, int stride) {
+    ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
+    nc = (n + CW - 1) / CW;      // column chunks
+    rg = first / nc;
+    c = first - rg * nc;
+    sq = stride / nc;
+    sr = stride - sq * nc;
+    skip();
+  }
+  __device__ __forceinline__ bool valid() const { return rg < ng; }
+  __device__ __forceinline__ void step() {
+    c += sr;
+    rg += sq;
+    if (c >= nc) {
+      c -= nc;
+      ++rg;
+    }
+  }
+  __device__ __forceinline__ void skip() {
+    while (rg < ng && (c + 1) * CW <= rg * DR + 1) step();
+  }
+  __device__ __forceinline__ void next() {
+    step();
+    skip();
+  }
+};
+
 template <typename WT>
 __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
     const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
-    const double* __restrict__ g64, const void* __restrict__ gest_v, int spin, SelGeom geo,
+    const double* __restrict__ g64, const void* __restrict__ gest_v,
+    const unsigned long long* __restrict__ parts, int nparts, int spin, SelGeom geo,
     unsigned long long* key, unsigned int* gthr, unsigned int* done, float* best_val,
     int* best_idx) {
   constexpr int VEC = 16 / (int)sizeof(WT);  // columns per consumer thread
@@ -432,19 +524,15 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
     s_fail = 0;
   }
   __syncthreads();
-  const int ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
-  const int nc = (n + CW - 1) / CW;      // column chunks
-  const int total = ng * nc;             // (n <= 46341: well inside int)
   uint64_t best = 0;
   if (warp == DS_CONSUMERS / 32) {
-    // producer: this CTA's tiles (a stride of gridDim.x over the rectangle of
-    // row groups x column chunks, tiles wholly at or below the diagonal
-    // skipped), each into the next stage once the consumers released it
+    // producer: this CTA's tiles, each into the next stage once the
+    // consumers released it. W is not written by the kernels before this
+    // one, so the copies start at once
     if (lane == 0) {
       int it = 0;
-      for (int tau = blockIdx.x; tau < total; tau += gridDim.x) {
-        const int rg = tau / nc, c = tau - rg * nc;
-        if ((c + 1) * CW <= rg * DR + 1) continue;
+      for (TileWalk<CW, DR> tw(n, blockIdx.x, gridDim.x); tw.valid(); tw.next()) {
+        const int rg = tw.rg, c = tw.c;
         const int st = it % DS_STAGES;
         const uint32_t use = (uint32_t)(it / DS_STAGES);
         if (use > 0 && !tc::mbar_wait(&empty_bar[st], (use - 1) & 1u)) {
@@ -469,41 +557,62 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
       }
     }
   } else {
-    // consumers: the same tiles in the same order; each tile's row gains and
-    // bits, this thread's column gains and bits and the threshold are loaded
-    // while the tile's copies land. The gains and the seeded threshold come
-    // from the kernels before this one: wait for them (the producer does not)
+    // consumers: wait for the kernels before this one (the gains in the
+    // estimate's type, the prep kernel's partials, the seeded threshold);
+    // the producer does not
     pdl_wait();
-    float thr = -INFINITY;
+    // the largest |gain| (every warp folds the prep kernel's partials itself)
+    uint64_t ga = 0;
+    for (int i = lane; i < nparts; i += 32) {
+      const uint64_t b = parts[nparts + i];
+      ga = b > ga ? b : ga;
+    }
+    ga = warp_max_u64(ga);
+    const float gabs = ga ? unord_f32((uint32_t)ga) : 0.0f;
+    float thr = thr_of(__ldcg(gthr));
+    // Each tile's row gains and bits, this thread's column gains and bits and
+    // the shared threshold are loaded one tile ahead, so their latency hides
+    // behind the tile before (the gains are padded: rows and columns past n
+    // read zeros)
+    ET fk[DR], fl[VEC];
+    uint32_t xk = 0, lw = 0;
+    unsigned int gt = 0;
+    TileWalk<CW, DR> tw(n, blockIdx.x, gridDim.x);
+    auto load_header = [&](int rg_, int c_) {
+      const int k0_ = rg_ * DR;
+#pragma unroll
+      for (int q = 0; q < DR / 4; ++q) {
+        const int4 v = __ldg(reinterpret_cast<const int4*>(gest + k0_) + q);
+        memcpy(&fk[4 * q], &v, 16);
+      }
+      xk = __ldg(theta + (k0_ >> 5)) >> (k0_ & 31);
+      const int l0_ = c_ * CW + (int)threadIdx.x * VEC;
+#pragma unroll
+      for (int q = 0; q < VEC / 4; ++q) {
+        const int4 v = __ldg(reinterpret_cast<const int4*>(gest + l0_) + q);
+        memcpy(&fl[4 * q], &v, 16);
+      }
+      lw = l0_ < n ? __ldg(theta + (l0_ >> 5)) >> (l0_ & 31) : 0u;
+      gt = __ldcg(gthr);
+    };
+    if (tw.valid()) load_header(tw.rg, tw.c);
     int it = 0;
-    for (int tau = blockIdx.x; tau < total; tau += gridDim.x) {
-      const int rg = tau / nc, c = tau - rg * nc;
-      if ((c + 1) * CW <= rg * DR + 1) continue;
+    while (tw.valid()) {
+      const int rg = tw.rg, c = tw.c;
       const int st = it % DS_STAGES;
       const uint32_t use = (uint32_t)(it / DS_STAGES);
       ++it;
       const int k0 = rg * DR;
-      ET fk[DR];
-      uint32_t xk = 0;
-      float gt = 0.0f;
-#pragma unroll
-      for (int i = 0; i < DR; ++i) {
-        const int k = min(k0 + i, n - 1);
-        fk[i] = __ldg(gest + k);
-        if constexpr (!INT) gt = fmaxf(gt, fabsf(fk[i]));
-        xk |= (uint32_t)get_bit32(theta, (uint32_t)k) << i;
-      }
       const int l0 = c * CW + (int)threadIdx.x * VEC;
-      ET fl[VEC];
-      float flmax = 0.0f;
-      const uint32_t lw = l0 < n ? __ldg(theta + (l0 >> 5)) >> (l0 & 31) : 0u;
+      ET fkc[DR], flc[VEC];
 #pragma unroll
-      for (int e = 0; e < VEC; ++e) {
-        const int l = l0 + e;
-        fl[e] = l < n ? __ldg(gest + l) : ET(0);
-        if constexpr (!INT) flmax = fmaxf(flmax, fabsf(fl[e]));
-      }
-      thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, __ldcg(gthr))));
+      for (int i = 0; i < DR; ++i) fkc[i] = fk[i];
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) flc[e] = fl[e];
+      const uint32_t xkc = xk, lwc = lw;
+      thr = fmaxf(thr, thr_of(max(*(volatile unsigned int*)&s_thr, gt)));
+      tw.next();
+      if (tw.valid()) load_header(tw.rg, tw.c);
       if (!tc::mbar_wait_warp(&full_bar[st], use & 1u)) {
         s_fail = 1;
         break;
@@ -515,65 +624,83 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
         const int4 v = *reinterpret_cast<const int4*>(tile + i * DS_ROW_BYTES);
         memcpy(&w[i][0], &v, 16);
       }
-      const float base = gt + flmax;
-      float cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
+      // |estimate - value| <= 2^-22 (|g_k| + |g_l| + |value|) <= 2^-22 (2 max|g| + |value|)
+      float cut = INT ? thr : thr - (2.0f * gabs + fabsf(thr)) * 9.5367431640625e-07f;
       int cut_i = thr > -INFINITY ? (int)thr : INT_MIN;
-      // (columns past the copied row segment hold stale bytes: such a thread
-      // has no column below n and skips the exact path)
-      bool any = false;
-      float ra[DR];  // float: each row's largest estimate
+      // each row's largest estimate f_k + max_l (f_l -/+ 2 W_kl) over this
+      // thread's columns. The coefficient of W_kl is -2 where the bits agree,
+      // else +2: for a row with bit 1 that is cp[e] (from column l's bit),
+      // for a row with bit 0 its negation. The rows' bits are the same for
+      // every thread, so the branch on them is uniform. (The grouping differs
+      // from the exact path's (f_k + f_l) -/+ 2 W by a few units in the last
+      // place, far inside the cut's 2^-20 margin.)
+      ET ra[DR];
+      bool any;
       if constexpr (INT) {
+        int cp[VEC];
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) cp[e] = ((lwc >> e) & 1u) ? -2 : 2;
+        int amax = INT_MIN;
 #pragma unroll
         for (int i = 0; i < DR; ++i) {
-          const uint32_t xki = (xk >> i) & 1u;
+          int r;
+          if ((xkc >> i) & 1u) {
+            r = flc[0] + cp[0] * (int)w[i][0];
 #pragma unroll
-          for (int e = 0; e < VEC; ++e) {
-            const int mm = -(int)(xki ^ ((lw >> e) & 1u));
-            const int wi = (int)w[i][e];
-            any |= fk[i] + fl[e] - 2 * ((wi ^ mm) - mm) >= cut_i;
-          }
-        }
-      } else {
-        // the largest estimate of the thread's pairs, f_k + (f_l -/+ 2 W).
-        // (The grouping differs from the exact path's (f_k + f_l) -/+ 2 W by
-        // a few units in the last place, far inside the cut's 2^-20 margin.)
-        // the coefficient of W_kl is -2 where the bits agree, else +2: for a
-        // row with bit 1 that is cp[e] (from column l's bit), for a row with
-        // bit 0 its negation. The rows' bits are the same for every thread,
-        // so the branch on them is uniform and each pair costs one FMA and
-        // one max.
-        float cp[VEC];
-#pragma unroll
-        for (int e = 0; e < VEC; ++e) cp[e] = ((lw >> e) & 1u) ? -2.0f : 2.0f;
-#pragma unroll
-        for (int i = 0; i < DR; ++i) {
-          float r;
-          if ((xk >> i) & 1u) {
-            r = fmaf(cp[0], w[i][0], fl[0]);
-#pragma unroll
-            for (int e = 1; e < VEC; ++e) r = fmaxf(r, fmaf(cp[e], w[i][e], fl[e]));
+            for (int e = 1; e < VEC; ++e) r = max(r, flc[e] + cp[e] * (int)w[i][e]);
           } else {
-            r = fmaf(-cp[0], w[i][0], fl[0]);
+            r = flc[0] - cp[0] * (int)w[i][0];
 #pragma unroll
-            for (int e = 1; e < VEC; ++e) r = fmaxf(r, fmaf(-cp[e], w[i][e], fl[e]));
+            for (int e = 1; e < VEC; ++e) r = max(r, flc[e] - cp[e] * (int)w[i][e]);
           }
-          ra[i] = fk[i] + r;
+          ra[i] = fkc[i] + r;
+          amax = max(amax, ra[i]);
         }
-        float amax = ra[0];
+        any = amax >= cut_i;
+      } else {
+        // two columns per packed f32x2 FMA
+        const float c0 = ((lwc >> 0) & 1u) ? -2.0f : 2.0f, c1 = ((lwc >> 1) & 1u) ? -2.0f : 2.0f;
+        const float c2 = ((lwc >> 2) & 1u) ? -2.0f : 2.0f, c3 = ((lwc >> 3) & 1u) ? -2.0f : 2.0f;
+        const uint64_t cp01 = pack2(c0, c1), cp23 = pack2(c2, c3);
+        const uint64_t cn01 = pack2(-c0, -c1), cn23 = pack2(-c2, -c3);
+        const uint64_t fl01 = pack2(flc[0], flc[1]), fl23 = pack2(flc[2], flc[3]);
 #pragma unroll
-        for (int i = 1; i < DR; ++i) amax = fmaxf(amax, ra[i]);
+        for (int i = 0; i < DR; ++i) {
+          const uint64_t w01 = pack2(w[i][0], w[i][1]), w23 = pack2(w[i][2], w[i][3]);
+          uint64_t d01, d23;
+          if ((xkc >> i) & 1u) {
+            d01 = fma2(cp01, w01, fl01);
+            d23 = fma2(cp23, w23, fl23);
+          } else {
+            d01 = fma2(cn01, w01, fl01);
+            d23 = fma2(cn23, w23, fl23);
+          }
+          float d0, d1, d2, d3;
+          unpack2(d01, d0, d1);
+          unpack2(d23, d2, d3);
+          ra[i] = fkc[i] + max3f(d0, d1, fmaxf(d2, d3));
+        }
+        float amax = max3f(ra[0], ra[1], ra[2]);
+#pragma unroll
+        for (int i = 3; i + 1 < DR; i += 2) amax = max3f(amax, ra[i], ra[i + 1]);
+        if constexpr (DR % 2 == 0) amax = fmaxf(amax, ra[DR - 1]);
         any = amax >= cut;
       }
       // (columns before the copied part hold stale bytes: every pair there
-      // has l <= k, and a thread with no column after the copy start has none)
+      // has l <= k, and a thread with no column after the copy start has
+      // none; columns past the copied row segment likewise: such a thread
+      // has no column below n)
       if (any && l0 < n && l0 + VEC > max(c * CW, (k0 + 1) & ~(VEC - 1))) {
-        const WT* tw = reinterpret_cast<const WT*>(ring + (size_t)st * DS_TILE_BYTES);
-        // float: only the rows whose largest estimate reaches the cut
-        uint32_t rows = (1u << DR) - 1u;
-        if constexpr (!INT) {
-          rows = 0u;
+        const WT* tw_ = reinterpret_cast<const WT*>(ring + (size_t)st * DS_TILE_BYTES);
+        // only the rows whose largest estimate reaches the cut
+        uint32_t rows = 0u;
 #pragma unroll
-          for (int i = 0; i < DR; ++i) rows |= (uint32_t)(ra[i] >= cut) << i;
+        for (int i = 0; i < DR; ++i) {
+          if constexpr (INT) {
+            rows |= (uint32_t)(ra[i] >= cut_i) << i;
+          } else {
+            rows |= (uint32_t)(ra[i] >= cut) << i;
+          }
         }
 #pragma unroll 1
         for (int b = 0; b < DR * VEC; ++b) {
@@ -584,8 +711,8 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
           }
           const int k = k0 + i, l = l0 + e;
           if (k >= n - 1 || l <= k || l >= n) continue;
-          const WT wv = tw[i * (DS_ROW_BYTES / (int)sizeof(WT)) + (l - c * CW)];
-          const uint32_t flip = (((xk >> i) & 1u) ^ ((lw >> e) & 1u)) ^ 1u;
+          const WT wv = tw_[i * (DS_ROW_BYTES / (int)sizeof(WT)) + (l - c * CW)];
+          const uint32_t flip = (((xkc >> i) & 1u) ^ ((lwc >> e) & 1u)) ^ 1u;
           float v;
           if constexpr (INT) {
             const int ai = __ldg(gest + k) + __ldg(gest + l) + (flip ? -2 * (int)wv : 2 * (int)wv);
@@ -604,7 +731,7 @@ __global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
           best = kk > best ? kk : best;
           if (kk != 0ull && vu > thr) {
             thr = vu;
-            cut = INT ? thr : thr - (base + fabsf(thr)) * 9.5367431640625e-07f;
+            cut = INT ? thr : thr - (2.0f * gabs + fabsf(thr)) * 9.5367431640625e-07f;
             cut_i = (int)thr;
           }
         }
@@ -968,7 +1095,7 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
   SelGeom geo;
   PQI_CHECK_ARG(make_sel_geom(combo, global_size, local_size, &geo));
   Workspace ws(workspace, workspace_bytes);
-  // key, the threshold word, the prep kernel's argmax key, the CTA counter
+  // the result key, the threshold word, a spare word, the CTA counter
   unsigned long long* key = ws.take<unsigned long long>(4);
   PQI_CHECK_ARG(key);
   cudaStream_t s = as_stream(stream);
@@ -979,44 +1106,48 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     if (rc) return rc;
     gains64 = g;
   }
-  // key (8 bytes), the shared threshold (4 bytes), the prep kernel's argmax
-  // and the stream kernel's CTA counter, zeroed together
-  PQI_TRY(cudaMemsetAsync(key, 0, 32, s));
-  unsigned int* gthr = reinterpret_cast<unsigned int*>(key + 1);
-  // the gains in the estimate's type (4 bytes each)
-  void* gest = ws.take<float>(n);
+  // the gains in the estimate's type (4 bytes each), padded for whole-vector
+  // reads, and the prep kernel's per-CTA partials
+  const int npad = (n + DS_GEST_PAD - 1) / DS_GEST_PAD * DS_GEST_PAD;
+  void* gest = ws.take<float>(npad);
   PQI_CHECK_ARG(gest);
-  const int pg = grid_for(n, 256, 148 * 4);
-  // the seed kernel and the pass are launched as programmatic dependents: the
-  // pass's producer streams W while the gains are converted and the
-  // threshold seeded; its consumers wait for both (pdl_wait)
+  const int pg = grid_for(npad, 256, 148);
+  unsigned long long* parts = ws.take<unsigned long long>(2 * (size_t)pg);
+  PQI_CHECK_ARG(parts);
+  // the result key, the shared threshold (key[1]) and the CTA counter
+  // (key[3]) are cleared by the prep kernel; the seed kernel and the pass
+  // are launched as programmatic dependents: the pass's producer streams W
+  // while the gains are converted and the threshold seeded, its consumers
+  // wait for both (pdl_wait)
+  unsigned int* gthr = reinterpret_cast<unsigned int*>(key + 1);
+  unsigned int* done = reinterpret_cast<unsigned int*>(key + 3);
+  const int i8 = w->kind == PQI_W_I8 ? 1 : 0;
   cudaLaunchAttribute pdl[1];
   pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   pdl[0].val.programmaticStreamSerializationAllowed = 1;
   cudaLaunchConfig_t seed_cfg = {};
-  seed_cfg.gridDim = dim3(pg);
+  seed_cfg.gridDim = dim3(grid_for(n, 256, 148 * 4));
   seed_cfg.blockDim = dim3(256);
   seed_cfg.stream = s;
   seed_cfg.attrs = pdl;
   seed_cfg.numAttrs = 1;
-  if (w->kind == PQI_W_I8) {
-    double_prep_kernel<int8_t><<<pg, 256, 0, s>>>(gains64, n, gest, key + 2);
+  if (i8) {
+    double_prep_kernel<int8_t><<<pg, 256, 0, s>>>(gains64, n, npad, gest, parts, key);
     PQI_LAUNCHED("double_prep_kernel");
-    PQI_TRY(cudaLaunchKernelEx(&seed_cfg, double_seed_kernel<int8_t>, (const int8_t*)w->W_i8, w->ld, n,
-                               theta, gains64, is_spin_glass, geo, (const unsigned long long*)(key + 2),
-                               key, gthr));
+    PQI_TRY(cudaLaunchKernelEx(&seed_cfg, double_seed_kernel<int8_t>, (const int8_t*)w->W_i8, w->ld,
+                               n, theta, gains64, is_spin_glass, geo,
+                               (const unsigned long long*)parts, pg, key, gthr));
   } else {
-    double_prep_kernel<float><<<pg, 256, 0, s>>>(gains64, n, gest, key + 2);
+    double_prep_kernel<float><<<pg, 256, 0, s>>>(gains64, n, npad, gest, parts, key);
     PQI_LAUNCHED("double_prep_kernel");
-    PQI_TRY(cudaLaunchKernelEx(&seed_cfg, double_seed_kernel<float>, (const float*)w->W_f32z, w->ld, n,
-                               theta, gains64, is_spin_glass, geo, (const unsigned long long*)(key + 2),
-                               key, gthr));
+    PQI_TRY(cudaLaunchKernelEx(&seed_cfg, double_seed_kernel<float>, (const float*)w->W_f32z, w->ld,
+                               n, theta, gains64, is_spin_glass, geo,
+                               (const unsigned long long*)parts, pg, key, gthr));
   }
   PQI_LAUNCHED("double_seed_kernel");
   // one persistent CTA per SM (the stage ring takes most of shared memory)
   static int sms = 0;
   static bool attr_set[2] = {false, false};
-  const int i8 = w->kind == PQI_W_I8 ? 1 : 0;
   if (!sms) {
     int dev = 0;
     PQI_TRY(cudaGetDevice(&dev));
@@ -1034,15 +1165,16 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
   cfg.stream = s;
   cfg.attrs = pdl;
   cfg.numAttrs = 1;
-  unsigned int* done = reinterpret_cast<unsigned int*>(key + 3);
   if (i8) {
     PQI_TRY(cudaLaunchKernelEx(&cfg, double_stream_kernel<int8_t>, (const int8_t*)w->W_i8, w->ld, n,
-                               theta, gains64, (const void*)gest, is_spin_glass, geo, key, gthr, done,
-                               best_energy, best_index));
+                               theta, gains64, (const void*)gest,
+                               (const unsigned long long*)parts, pg, is_spin_glass, geo, key, gthr,
+                               done, best_energy, best_index));
   } else {
     PQI_TRY(cudaLaunchKernelEx(&cfg, double_stream_kernel<float>, (const float*)w->W_f32z, w->ld, n,
-                               theta, gains64, (const void*)gest, is_spin_glass, geo, key, gthr, done,
-                               best_energy, best_index));
+                               theta, gains64, (const void*)gest,
+                               (const unsigned long long*)parts, pg, is_spin_glass, geo, key, gthr,
+                               done, best_energy, best_index));
   }
   PQI_LAUNCHED("double_stream_kernel");
   return PQI_OK;
