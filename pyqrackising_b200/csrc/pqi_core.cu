@@ -422,6 +422,7 @@ constexpr int DS_THREADS = DS_CONSUMERS + 32;
 constexpr int DS_ROW_BYTES = 16 * DS_CONSUMERS;  // 4 KB of a row per tile
 constexpr int DS_TILE_BYTES = DS_ROWS * DS_ROW_BYTES;
 constexpr int DS_SMEM = DS_STAGES * DS_TILE_BYTES;
+constexpr int DS_CTAS_PER_SM = 1;  // resident pass CTAs per SM
 // the gains in the estimate's type are padded to a multiple of this many
 // entries (a whole tile's columns for either weight type)
 constexpr int DS_GEST_PAD = 4096;
@@ -456,43 +457,58 @@ __device__ __forceinline__ float max3f(float a, float b, float c) {
   return d;
 }
 
-// The pass's tiles: the rectangle of row groups x column chunks in row group
-// major order, every CTA taking tiles b, b + gridDim.x, ... and skipping those
-// wholly at or below the diagonal ((c + 1) CW <= rg DR + 1). The producer and
-// the consumers walk the same sequence; a step is a few adds (the stride's
-// quotient and remainder by the chunk count are taken once).
+// The pass's tiles: the kept tiles (those reaching above the diagonal,
+// (c + 1) CW > rg DR + 1, i.e. chunks c >= rg / (CW / DR) of row group rg) in
+// row group major order, cut into gridDim.x contiguous runs, one per CTA.
+// Each CTA so streams its own rows chunk after chunk, and at any time the
+// CTAs read rows spread over the whole triangle (measured faster than
+// interleaving the CTAs tile by tile). The start of a run is found by a
+// binary search on the closed-form count of kept tiles before a row group.
+// The producer and the consumers walk the same run.
 template <int CW, int DR>
 struct TileWalk {
-  int ng, nc, rg, c, sq, sr;
-  __device__ __forceinline__ TileWalk(int n, int first, int stride) {
-    ng = (n - 1 + DR - 1) / DR;  // row groups over rows 0 .. n-2
-    nc = (n + CW - 1) / CW;      // column chunks
-    rg = first / nc;
-    c = first - rg * nc;
-    sq = stride / nc;
-    sr = stride - sq * nc;
-    skip();
+  int ng, nc, rg, c, left;
+  // kept tiles of row groups 0 .. R-1 (row group r keeps chunks r / Q .. nc-1)
+  __device__ __forceinline__ long long prefix(long long R) const {
+    constexpr long long Q = CW / DR;
+    const long long a = R / Q, r = R - (R / Q) * Q;
+    return R * nc - (Q * a * (a - 1) / 2 + a * r);
   }
-  __device__ __forceinline__ bool valid() const { return rg < ng; }
-  __device__ __forceinline__ void step() {
-    c += sr;
-    rg += sq;
-    if (c >= nc) {
-      c -= nc;
-      ++rg;
+  __device__ __forceinline__ TileWalk(int n, int b, int G) {
+    ng = (n - 1 + DR - 1) / DR;
+    nc = (n + CW - 1) / CW;
+    const long long total = prefix(ng);
+    const long long T = (total + G - 1) / G;
+    const long long t0 = (long long)b * T;
+    const long long t1 = t0 + T < total ? t0 + T : total;
+    left = t1 > t0 ? (int)(t1 - t0) : 0;
+    rg = ng;
+    c = 0;
+    if (!left) return;
+    int lo = 0, hi = ng - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix(mid) <= t0) {
+        lo = mid;
+      } else {
+        hi = mid - 1;
+      }
     }
+    rg = lo;
+    c = rg / (CW / DR) + (int)(t0 - prefix(rg));
   }
-  __device__ __forceinline__ void skip() {
-    while (rg < ng && (c + 1) * CW <= rg * DR + 1) step();
-  }
+  __device__ __forceinline__ bool valid() const { return left > 0; }
   __device__ __forceinline__ void next() {
-    step();
-    skip();
+    --left;
+    if (++c == nc) {
+      ++rg;
+      c = rg / (CW / DR);
+    }
   }
 };
 
 template <typename WT>
-__global__ void __launch_bounds__(DS_THREADS, 1) double_stream_kernel(
+__global__ void __launch_bounds__(DS_THREADS, DS_CTAS_PER_SM) double_stream_kernel(
     const WT* __restrict__ Wp, int ld, int n, const uint32_t* __restrict__ theta,
     const double* __restrict__ g64, const void* __restrict__ gest_v,
     const unsigned long long* __restrict__ parts, int nparts, int spin, SelGeom geo,
@@ -1145,7 +1161,8 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
                                (const unsigned long long*)parts, pg, key, gthr));
   }
   PQI_LAUNCHED("double_seed_kernel");
-  // one persistent CTA per SM (the stage ring takes most of shared memory)
+  // persistent CTAs, DS_CTAS_PER_SM per SM (the stage rings take most of
+  // shared memory)
   static int sms = 0;
   static bool attr_set[2] = {false, false};
   if (!sms) {
@@ -1159,7 +1176,7 @@ pqi_status pqi_double_bit_flips(const pqi_weights* w, const uint32_t* theta,
     attr_set[i8] = true;
   }
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(sms);
+  cfg.gridDim = dim3(sms * DS_CTAS_PER_SM);
   cfg.blockDim = dim3(DS_THREADS);
   cfg.dynamicSmemBytes = DS_SMEM;
   cfg.stream = s;
