@@ -380,6 +380,13 @@ pqi_status pqi_batch_search_cta(const void* graphs, int num_graphs, const int* t
  * every row group in registers. Results are identical. */
 pqi_status pqi_batch_set_staging(int on);
 
+/* Tuning / cross-check knob (no reference counterpart): on (default) lets
+ * pqi_batch_search (float64 local fields, CTA form) keep the fields of float
+ * graphs of 4097 to 8192 nodes in tensor memory, four tasks per SM, each
+ * flip's row fetched whole by one bulk copy; off keeps them in shared memory
+ * (three tasks per SM). Results are identical. */
+pqi_status pqi_batch_set_tmem_fields(int on);
+
 /* Cross-check knob (no reference counterpart): on (default) the batched
  * searches and the cluster ascent of graphs of 64 nodes or more compute the
  * starting local fields of all dense-graph tasks first, one pass over W per

@@ -133,6 +133,7 @@ SIGNATURES = {
     "pqi_tfim_jz": (_i, [_vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_tfim_jz_f32": (_i, [_vp, _i, _vp, _vp, _vp, _sz, _vp]),
     "pqi_batch_set_staging": (_i, [_i]),
+    "pqi_batch_set_tmem_fields": (_i, [_i]),
     "pqi_batch_set_start_pass": (_i, [_i]),
     "pqi_bnb_eval": (_i, [_vp, _i, _vp, _i, ctypes.c_double, _i, _vp, _vp, _vp, _vp, _vp]),
     "pqi_coo_to_dense": (_i, [_vp, _vp, _vp, ctypes.c_longlong, _i, _vp, _vp, _vp, _vp]),

@@ -22,6 +22,7 @@
 #include <type_traits>
 
 #include "pqi_common.cuh"
+#include "pqi_tc.cuh"
 
 namespace pqi {
 
@@ -631,6 +632,318 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
 }
 
 // ---------------------------------------------------------------------------
+// Float64 local fields in tensor memory (float weights, 4096 < n <= 8192).
+//
+// The shared-memory form holds a task's float64 fields in shared memory:
+// 64 KB at n = 8192, three tasks per SM, and each flip streams its 32 KB row in
+// two register chunks. Here the fields live in the SM's tensor memory (TMEM,
+// 128 lanes x 512 columns of 32 bits): a CTA of 128 threads allocates 128
+// columns, thread t keeps its 64 nodes' fields in its own lane (node
+// v = 4 t + 512 j + i at columns 2 (4 j + i) and 2 (4 j + i) + 1), four tasks
+// per SM share the 512 columns, and shared memory is left for the flipped row:
+// one bulk copy of the whole row per flip (mbarrier completion). A flip pass
+// moves the fields through registers 32 columns (16 nodes) at a time with
+// tcgen05.ld / tcgen05.st; the arithmetic, the selection (float gain, lowest
+// node, the node's bit) and the float64 running value are those of the
+// shared-memory form, so both return the same states, values and flip counts.
+// Each CTA asks for enough shared memory that a fifth CTA cannot join an SM
+// whose TMEM four CTAs hold.
+constexpr int TM_BT = 128;
+constexpr int TM_J = 16;                         // groups of four nodes per thread
+constexpr int TM_NMAX = 4 * TM_BT * TM_J;        // 8192 nodes
+constexpr int TM_COLS = 2 * 4 * TM_J;            // 128 columns per CTA
+constexpr int TM_STAGE_BYTES = TM_NMAX * 4;      // one float32 row
+constexpr int TM_SMEM_MIN = 50 * 1024;           // > 228 KB / 5: at most four CTAs per SM
+
+__device__ __forceinline__ void tm_st32(uint32_t taddr, const uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, "
+      "%17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]),
+      "r"(r[8]), "r"(r[9]), "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]),
+      "r"(r[15]), "r"(r[16]), "r"(r[17]), "r"(r[18]), "r"(r[19]), "r"(r[20]), "r"(r[21]),
+      "r"(r[22]), "r"(r[23]), "r"(r[24]), "r"(r[25]), "r"(r[26]), "r"(r[27]), "r"(r[28]),
+      "r"(r[29]), "r"(r[30]), "r"(r[31])
+      : "memory");
+}
+__device__ __forceinline__ void tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ double tm_ld_f64(uint32_t taddr) {
+  uint32_t lo, hi;
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];" : "=r"(lo), "=r"(hi) : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+  return __hiloint2double((int)hi, (int)lo);
+}
+
+struct TmCtx {
+  const float* W;
+  int n, ld;
+  uint32_t* bits;
+  const float* stage;  // the flipped row (shared memory)
+  uint32_t tbase;      // this warp's lanes, column 0 of the CTA's allocation
+};
+
+// One flip pass of the TMEM form: with k >= 0 the row k is in the stage,
+// flip k (coefficient -2 x_k) in this thread's fields and bits; then the
+// CTA's best key and the selected node's exact gain (as flip_and_select).
+template <bool UPD>
+__device__ __forceinline__ void tm_pass(const TmCtx& c, int k, int xk,
+                                        unsigned long long (*red_key)[4], double (*red_y)[4],
+                                        int par, unsigned long long* out_key, double* out_g) {
+  const int t = threadIdx.x, n = c.n;
+  const double coef = xk ? -2.0 : 2.0;
+  float bv = -INFINITY;
+  int bi = -1;
+  double by = 0.0;
+#pragma unroll 1
+  for (int q = 0; q < TM_J / 4; ++q) {
+    if (2048 * q >= n) break;  // (uniform: no node of this chunk below n)
+    uint32_t r[32];
+    tc::tmem_load32(c.tbase + 32u * q, r);
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      const int v0 = 4 * t + 512 * (4 * q + jj);
+      if (v0 >= n) continue;
+      float w4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+      if (UPD) {
+        const float4 s4 = *reinterpret_cast<const float4*>(c.stage + v0);
+        w4[0] = s4.x; w4[1] = s4.y; w4[2] = s4.z; w4[3] = s4.w;
+        if ((unsigned)(k - v0) < 4u) c.bits[k >> 5] ^= 1u << (k & 31);
+      }
+      const uint32_t nib = c.bits[v0 >> 5] >> (v0 & 31);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (v0 + i < n) {
+          const int s = 8 * jj + 2 * i;
+          double y = __hiloint2double((int)r[s + 1], (int)r[s]);
+          if (UPD) {
+            y += coef * (double)w4[i];
+            r[s] = (uint32_t)__double2loint(y);
+            r[s + 1] = (uint32_t)__double2hiint(y);
+          }
+          const float yf = (float)y;
+          const float gv = ((nib >> i) & 1u) ? yf : -yf;
+          if (gv > bv) {
+            bv = gv;
+            bi = v0 + i;
+            by = y;
+          }
+        }
+      }
+    }
+    if (UPD) tm_st32(c.tbase + 32u * q, r);
+  }
+  if (UPD) tm_wait_st();
+  const int lane = t & 31, warp = t >> 5;
+  const int bx = bi >= 0 ? (int)((c.bits[bi >> 5] >> (bi & 31)) & 1u) : 0;
+  const unsigned long long key = bi >= 0 ? bkey(bv, bi, bx) : 0ull;
+  const unsigned long long wk = bmax_key(key);
+  const uint32_t src = __ballot_sync(0xFFFFFFFFu, key == wk && wk != 0ull);
+  if (lane == (src ? __ffs(src) - 1 : 0)) {
+    red_key[par][warp] = wk;
+    red_y[par][warp] = by;
+  }
+  __syncthreads();
+  const unsigned long long sk = lane < 4 ? red_key[par][lane] : 0ull;
+  const unsigned long long gk = bmax_key(sk);
+  const uint32_t ws = __ballot_sync(0xFFFFFFFFu, lane < 4 && sk == gk && gk != 0ull);
+  double g_win = 0.0;
+  if (gk != 0ull) {
+    const double y = red_y[par][__ffs(ws) - 1];
+    g_win = (gk & 1ull) ? y : -y;
+  }
+  *out_g = g_win;
+  *out_key = gk;
+}
+
+__global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
+    const BatchGraph* __restrict__ graphs, const int* __restrict__ task_graph,
+    const uint32_t* __restrict__ init_states, int words_pitch, int tasks, int spin, int rounds,
+    int kick, int flip_budget, uint64_t seed, const double* __restrict__ kick_cdf,
+    const long long* __restrict__ cdf_offset, uint32_t* __restrict__ best_states,
+    double* __restrict__ best_values, unsigned long long* __restrict__ flips_total,
+    int* __restrict__ status, const double* __restrict__ start_fields, int fields_pitch) {
+  extern __shared__ __align__(16) unsigned char tm_smem[];
+  __shared__ double red[4];
+  __shared__ unsigned long long red_key[2][4];
+  __shared__ double red_y[2][4];
+  __shared__ __align__(8) uint64_t row_bar;
+  __shared__ uint32_t s_tmem;
+  __shared__ double s_pub;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  float* stage = reinterpret_cast<float*>(tm_smem);
+  uint32_t* bits = reinterpret_cast<uint32_t*>(tm_smem + TM_STAGE_BYTES);
+  uint32_t* kicked = bits + TM_NMAX / 32;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32(&s_tmem)),
+                 "r"(TM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) {
+    tc::mbar_init(&row_bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  uint32_t phase = 0;
+  bool failed = false;
+  for (int task = blockIdx.x; task < tasks && !failed; task += gridDim.x) {
+    const BatchGraph G = graphs[task_graph[task]];
+    const int n = G.n, n32 = (n + 31) >> 5;
+    TmCtx c;
+    c.W = static_cast<const float*>(G.W);
+    c.n = n;
+    c.ld = G.ld;
+    c.bits = bits;
+    c.stage = stage;
+    c.tbase = s_tmem + ((uint32_t)(32 * warp) << 16);
+    uint32_t* best_bits = best_states + (size_t)task * words_pitch;
+    for (int w = t; w < n32; w += TM_BT) bits[w] = init_states[(size_t)task * words_pitch + w];
+    __syncthreads();
+    // 1. starting fields of this thread's own nodes (from the start pass, or
+    // summed over the node's row list), stored to TMEM 16 nodes at a time;
+    // x_v y_v into this thread's share of q = x^T W x
+    double qpart = 0.0;
+    const double* __restrict__ yrow =
+        (start_fields && !G.adj_ptr) ? start_fields + (size_t)task * fields_pitch : nullptr;
+#pragma unroll 1
+    for (int q = 0; q < TM_J / 4; ++q) {
+      uint32_t r[32];
+#pragma unroll
+      for (int s = 0; s < 16; ++s) {
+        const int v = 4 * t + 512 * (4 * q + (s >> 2)) + (s & 3);
+        double y = 0.0;
+        if (v < n) {
+          if (yrow) {
+            y = yrow[v];
+          } else {
+            const long long e1 = G.adj_ptr[v + 1];
+            for (long long e = G.adj_ptr[v]; e < e1; ++e) {
+              const int u = G.adj_col[e];
+              if (u == v) continue;
+              const double w = (double)G.adj_val[e];
+              y += ((bits[u >> 5] >> (u & 31)) & 1) ? w : -w;
+            }
+          }
+          qpart += ((bits[v >> 5] >> (v & 31)) & 1) ? y : -y;
+        }
+        r[2 * s] = (uint32_t)__double2loint(y);
+        r[2 * s + 1] = (uint32_t)__double2hiint(y);
+      }
+      tm_st32(c.tbase + 32u * q, r);
+    }
+    tm_wait_st();
+    for (int o = 16; o > 0; o >>= 1) qpart += __shfl_xor_sync(0xFFFFFFFFu, qpart, o);
+    if (lane == 0) red[warp] = qpart;
+    __syncthreads();
+    const double qv = red[0] + red[1] + red[2] + red[3];
+    const double scale = spin ? 2.0 : 1.0;
+    double val = spin ? -qv / 2.0 : (2.0 * G.upper_sum - qv) / 4.0;
+    double best = -INFINITY;
+    unsigned long long nflips = 0;
+    int timeout = 0;
+    unsigned long long key;
+    double gk;
+    int par = 0;
+    // the row of node k into the stage by one bulk copy (every thread has
+    // finished reading the previous row: the pass before ended on a CTA
+    // barrier)
+    auto flip = [&](int k, int xk) -> bool {
+      if (t == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint32_t bytes = (uint32_t)(((n + 3) & ~3) * 4);
+        tc::mbar_expect_tx(&row_bar, bytes);
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                tc::smem_u32(stage)),
+            "l"(c.W + (size_t)k * c.ld), "r"(bytes), "r"(tc::smem_u32(&row_bar))
+            : "memory");
+      }
+      // (one lane per warp waits, bounded; the CTA then agrees, so a wait
+      // that ran out anywhere stops the task everywhere)
+      bool ok = true;
+      if (lane == 0) ok = tc::mbar_wait_spin(&row_bar, phase);
+      ok = __syncthreads_and(ok ? 1 : 0) != 0;
+      phase ^= 1u;
+      if (!ok) return false;
+      tm_pass<true>(c, k, xk, red_key, red_y, par, &key, &gk);
+      par ^= 1;
+      return true;
+    };
+    tm_pass<false>(c, -1, 0, red_key, red_y, par, &key, &gk);
+    par ^= 1;
+    for (int r = 0; r <= rounds && !failed; ++r) {
+      for (int f = 0;; ++f) {
+        if (key == 0ull || !(unord_f32((uint32_t)(key >> 32)) > 0.0f)) break;
+        if (f >= flip_budget) {
+          timeout = 1;
+          break;
+        }
+        const int k = (int)(0x3FFFFFFFu - (((uint32_t)key) >> 1));
+        const int xk = (int)(key & 1ull);
+        const double gprev = gk;
+        if (!flip(k, xk)) {
+          failed = true;
+          break;
+        }
+        val += scale * gprev;
+        ++nflips;
+      }
+      if (failed) break;
+      if (val > best) {
+        best = val;
+        for (int w = t; w < n32; w += TM_BT) best_bits[w] = bits[w];
+      }
+      if (r == rounds) break;
+      for (int w = t; w < n32; w += TM_BT) kicked[w] = 0u;
+      __syncthreads();
+      for (int j = 0; j < kick; ++j) {
+        int pick = 0;
+        for (int attempt = 0; attempt < 16; ++attempt) {
+          const double u =
+              bunif(seed, (uint64_t)task * 1315423911ull + r, (uint64_t)j + ((uint64_t)attempt << 20));
+          pick = draw_node(u, n, kick_cdf ? kick_cdf + cdf_offset[task_graph[task]] : nullptr);
+          if (!((kicked[pick >> 5] >> (pick & 31)) & 1u)) break;
+        }
+        const int xp = (bits[pick >> 5] >> (pick & 31)) & 1;
+        // the kicked node's field, from its owner's lane
+        const int owner = (pick >> 2) & (TM_BT - 1);
+        if (warp == owner >> 5) {
+          const int s = 4 * (pick / 512) + (pick & 3);
+          const double y = tm_ld_f64(c.tbase + 2u * s);
+          if (lane == (owner & 31)) s_pub = y;
+        }
+        __syncthreads();  // everyone has read bit, field and kicked set before they change
+        const double gp = xp ? s_pub : -s_pub;
+        if (t == 0) kicked[pick >> 5] |= 1u << (pick & 31);
+        if (!flip(pick, xp)) {
+          failed = true;
+          break;
+        }
+        val += scale * gp;
+        ++nflips;
+      }
+    }
+    if (t == 0) {
+      best_values[task] = best;
+      atomicAdd(flips_total, nflips);
+      if (timeout) atomicExch(status, PQI_ETIMEOUT);
+      if (failed) atomicExch(status, PQI_ETIMEOUT);
+    }
+    __syncthreads();
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(TM_COLS)
+                 : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Warp-per-task form for small graphs (n <= 128 * NG): the same search, the
 // same selection rule and the same kick stream as batch_search_kernel, with
 // one warp per task and no shared memory. Lane l owns the nodes
@@ -850,6 +1163,7 @@ size_t pqi_batch_graph_desc_bytes(void) { return sizeof(BatchGraph); }
 }  // extern "C"
 
 static int g_batch_no_stage = 0;
+static int g_batch_no_tmem = 0;
 static int g_batch_no_start_pass = 0;
 
 // Starting fields of the dense-graph tasks (start_fields_kernel) into a
@@ -932,6 +1246,30 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   pqi_status sfst = start_fields(gd, task_graph, init_states, words_pitch, tasks, max_n, i8, s, &sf,
                                  &sf_pitch);
   if (sfst != PQI_OK) return sfst;
+  // float weights with float64 fields and 4096 < n <= 8192: the fields in
+  // tensor memory (four tasks per SM, each flip's whole row in one bulk copy)
+  if (!i8 && !f32 && bt == 256 && max_n > 4096 && max_n <= TM_NMAX && sf && !g_batch_no_tmem) {
+    const size_t tsm = std::max((size_t)TM_SMEM_MIN, (size_t)TM_STAGE_BYTES + TM_NMAX / 4);
+    PQI_TRY(cudaFuncSetAttribute(batch_search_tmem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tsm));
+    PQI_TRY(cudaFuncSetAttribute(batch_search_tmem_kernel,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    // resident CTAs per SM: four by shared memory and registers, and four
+    // allocations of TM_COLS fill the 512 TMEM columns (the occupancy query
+    // reports one CTA per SM for a kernel that allocates tensor memory)
+    int tper = 0;
+    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tper, batch_search_tmem_kernel, TM_BT, tsm));
+    if (tper >= 1) {
+      tper = 512 / TM_COLS;
+      const int grid = std::max(1, std::min(tasks, num_sms * tper));
+      batch_search_tmem_kernel<<<grid, TM_BT, tsm, s>>>(
+          gd, task_graph, init_states, words_pitch, tasks, is_spin_glass, rounds, kick, flip_budget,
+          seed, kick_cdf, cdf_offset, best_states, best_values, flips_total, status, sf, sf_pitch);
+      PQI_LAUNCHED("batch_search_tmem_kernel");
+      PQI_TRY(cudaFreeAsync(sf, s));
+      return PQI_OK;
+    }
+  }
   // row loads per thread: groups of four nodes, CH groups in flight per chunk
   // (the whole row for n <= 4 * 256 * CH). CH = 4 keeps three CTAs per SM
   // within the register file (8 groups spill at that occupancy and run slower
@@ -1026,6 +1364,11 @@ pqi_status pqi_batch_set_start_pass(int on) {
 
 pqi_status pqi_batch_set_staging(int on) {
   g_batch_no_stage = on ? 0 : 1;
+  return PQI_OK;
+}
+
+pqi_status pqi_batch_set_tmem_fields(int on) {
+  g_batch_no_tmem = on ? 0 : 1;
   return PQI_OK;
 }
 

@@ -71,6 +71,33 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   }
 }
 
+// mbar_wait without the suspend hint: each try_wait returns after the
+// hardware's own short time limit, so a thread waiting on a phase that
+// completes in a microsecond or two resumes as soon as it completes.
+__device__ __forceinline__ bool mbar_wait_spin(uint64_t* bar, uint32_t parity) {
+  const uint32_t addr = smem_u32(bar);
+  long long t0 = 0;
+  for (uint32_t iter = 0;; ++iter) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(addr), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((iter & 63u) == 0u) {
+      const long long now = clock64();
+      if (iter == 0u) {
+        t0 = now;
+      } else if (now - t0 > WAIT_BUDGET_CYCLES) {
+        return false;
+      }
+    }
+  }
+}
+
 // mbar_wait by lane 0 of the calling warp only; every lane gets the result.
 // The lanes' later shared-memory accesses are ordered after the wait by the
 // warp synchronisation.

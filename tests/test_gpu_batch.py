@@ -306,6 +306,39 @@ def test_float32_fields_staged_rows_match_register_rows():
         assert np.all(x * (W @ x) <= 1e-5 * np.abs(W).sum(axis=1).max())
 
 
+def test_tmem_fields_match_shared_memory_fields():
+    """Float64 fields in tensor memory (float graphs of 4097-8192 nodes, four
+    tasks per SM) give the same states, values and flip counts as the fields
+    in shared memory, for dense graphs (starting fields from the start pass)
+    and row-list graphs (summed by each field's owner), with kicks; the states
+    are local optima of the float64 objective."""
+    from pyqrackising_b200 import _lib
+    from pyqrackising_b200 import workloads as wl
+    from pyqrackising_b200.batch import BatchedSearch
+    from pyqrackising_b200.device import DeviceGraph
+
+    Ws = [wl.sherrington_kirkpatrick(8192, seed=31), wl.gnp_weighted(5000, 0.02, seed=32, dist="normal"),
+          wl.gnp_weighted(4500, 0.3, seed=33, dist="uniform")]
+    bs = BatchedSearch([DeviceGraph(W) for W in Ws])
+    task_graph = [0, 1, 2, 0, 1, 2, 0]
+    words = bs.random_states(task_graph, seed=8)
+    try:
+        _lib.call("pqi_batch_set_tmem_fields", 0)
+        va, ba, fa, sa = bs.run(task_graph, words, True, rounds=2, kick=6, seed=4)
+        _lib.call("pqi_batch_set_tmem_fields", 1)
+        vb, bb, fb, sb = bs.run(task_graph, words, True, rounds=2, kick=6, seed=4)
+    finally:
+        _lib.call("pqi_batch_set_tmem_fields", 1)
+    assert int(sa.item()) == 0 and int(sb.item()) == 0
+    assert torch.equal(ba, bb) and torch.equal(va, vb) and int(fa.item()) == int(fb.item())
+    for t, g in enumerate(task_graph[:3]):
+        bits = bs.unpack(bb, task_graph)[t]
+        W = Ws[g].astype(np.float64)
+        np.fill_diagonal(W, 0.0)
+        x = np.where(bits, 1.0, -1.0)
+        assert float(vb[t]) == pytest.approx(-0.5 * x @ W @ x, rel=1e-9)
+
+
 @pytest.mark.parametrize("kind", ["int", "float"])
 def test_cta128_form_matches_cta_form(kind):
     """The 128-thread CTA form (pqi_batch_search_cta) follows the 256-thread
