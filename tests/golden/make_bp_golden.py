@@ -1,6 +1,7 @@
 """Golden marginals of the reference's belief propagation
 (pyqrackising/spin_glass_solver.py:311-415), generated by importing the
-reference in the build container (PYTHONPATH=/root/reference):
+reference in the build container (its checkout: $PQI_REFERENCE_ROOT, else
+/root/reference):
 
     python tests/golden/make_bp_golden.py
 
@@ -12,7 +13,7 @@ import sys
 
 import numpy as np
 
-sys.path.insert(0, "/root/reference")
+sys.path.insert(0, os.environ.get("PQI_REFERENCE_ROOT", "/root/reference"))
 import importlib  # noqa: E402
 
 ref = importlib.import_module("pyqrackising.spin_glass_solver")

@@ -1,5 +1,6 @@
 """Golden vectors of the reference's sparse path, generated by importing the
-reference in the build container (PYTHONPATH=/root/reference):
+reference in the build container (its checkout: $PQI_REFERENCE_ROOT, else
+/root/reference):
 
     python tests/golden/make_sparse_golden.py
 
@@ -16,7 +17,7 @@ import sys
 import numpy as np
 from scipy.sparse import csr_matrix
 
-sys.path.insert(0, "/root/reference")
+sys.path.insert(0, os.environ.get("PQI_REFERENCE_ROOT", "/root/reference"))
 ms = importlib.import_module("pyqrackising.maxcut_tfim_sparse")
 mu = importlib.import_module("pyqrackising.maxcut_tfim_util")
 
