@@ -684,17 +684,18 @@ struct TmCtx {
 };
 
 // One flip pass of the TMEM form: with k >= 0 the row k is in the stage,
-// flip k (coefficient -2 x_k) in this thread's fields and bits; then the
-// CTA's best key and the selected node's exact gain (as flip_and_select).
+// flip k (coefficient -2 x_k) in this thread's fields and bits, and return in
+// *out_gk the exact gain of k before the flip (its field is unchanged by its
+// own flip, W_kk = 0: the owner warp reads it back once instead of every
+// thread keeping the field of its best node); then the CTA's best key.
 template <bool UPD>
 __device__ __forceinline__ void tm_pass(const TmCtx& c, int k, int xk,
-                                        unsigned long long (*red_key)[4], double (*red_y)[4],
-                                        int par, unsigned long long* out_key, double* out_g) {
+                                        unsigned long long (*red_key)[4], double* s_yk, int par,
+                                        unsigned long long* out_key, double* out_gk) {
   const int t = threadIdx.x, n = c.n;
   const double coef = xk ? -2.0 : 2.0;
   float bv = -INFINITY;
   int bi = -1;
-  double by = 0.0;
 #pragma unroll 1
   for (int q = 0; q < TM_J / 4; ++q) {
     if (2048 * q >= n) break;  // (uniform: no node of this chunk below n)
@@ -726,34 +727,30 @@ __device__ __forceinline__ void tm_pass(const TmCtx& c, int k, int xk,
           if (gv > bv) {
             bv = gv;
             bi = v0 + i;
-            by = y;
           }
         }
       }
     }
     if (UPD) tm_st32(c.tbase + 32u * q, r);
   }
-  if (UPD) tm_wait_st();
   const int lane = t & 31, warp = t >> 5;
+  if (UPD) {
+    tm_wait_st();
+    const int owner = (k >> 2) & (TM_BT - 1);
+    if (warp == owner >> 5) {
+      const double y = tm_ld_f64(c.tbase + 2u * (uint32_t)(4 * (k / 512) + (k & 3)));
+      if (lane == (owner & 31)) s_yk[par] = y;
+    }
+  }
   const int bx = bi >= 0 ? (int)((c.bits[bi >> 5] >> (bi & 31)) & 1u) : 0;
   const unsigned long long key = bi >= 0 ? bkey(bv, bi, bx) : 0ull;
   const unsigned long long wk = bmax_key(key);
   const uint32_t src = __ballot_sync(0xFFFFFFFFu, key == wk && wk != 0ull);
-  if (lane == (src ? __ffs(src) - 1 : 0)) {
-    red_key[par][warp] = wk;
-    red_y[par][warp] = by;
-  }
+  if (lane == (src ? __ffs(src) - 1 : 0)) red_key[par][warp] = wk;
   __syncthreads();
   const unsigned long long sk = lane < 4 ? red_key[par][lane] : 0ull;
-  const unsigned long long gk = bmax_key(sk);
-  const uint32_t ws = __ballot_sync(0xFFFFFFFFu, lane < 4 && sk == gk && gk != 0ull);
-  double g_win = 0.0;
-  if (gk != 0ull) {
-    const double y = red_y[par][__ffs(ws) - 1];
-    g_win = (gk & 1ull) ? y : -y;
-  }
-  *out_g = g_win;
-  *out_key = gk;
+  *out_key = bmax_key(sk);
+  if (UPD) *out_gk = xk ? s_yk[par] : -s_yk[par];
 }
 
 __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
@@ -766,10 +763,9 @@ __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
   extern __shared__ __align__(16) unsigned char tm_smem[];
   __shared__ double red[4];
   __shared__ unsigned long long red_key[2][4];
-  __shared__ double red_y[2][4];
+  __shared__ double s_yk[2];
   __shared__ __align__(8) uint64_t row_bar;
   __shared__ uint32_t s_tmem;
-  __shared__ double s_pub;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   float* stage = reinterpret_cast<float*>(tm_smem);
   uint32_t* bits = reinterpret_cast<uint32_t*>(tm_smem + TM_STAGE_BYTES);
@@ -846,7 +842,7 @@ __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
     unsigned long long nflips = 0;
     int timeout = 0;
     unsigned long long key;
-    double gk;
+    double gflip = 0.0;  // the gain of the node the last pass flipped, before the flip
     int par = 0;
     // the row of node k into the stage by one bulk copy (every thread has
     // finished reading the previous row: the pass before ended on a CTA
@@ -869,11 +865,11 @@ __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
       ok = __syncthreads_and(ok ? 1 : 0) != 0;
       phase ^= 1u;
       if (!ok) return false;
-      tm_pass<true>(c, k, xk, red_key, red_y, par, &key, &gk);
+      tm_pass<true>(c, k, xk, red_key, s_yk, par, &key, &gflip);
       par ^= 1;
       return true;
     };
-    tm_pass<false>(c, -1, 0, red_key, red_y, par, &key, &gk);
+    tm_pass<false>(c, -1, 0, red_key, s_yk, par, &key, &gflip);
     par ^= 1;
     for (int r = 0; r <= rounds && !failed; ++r) {
       for (int f = 0;; ++f) {
@@ -884,12 +880,11 @@ __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
         }
         const int k = (int)(0x3FFFFFFFu - (((uint32_t)key) >> 1));
         const int xk = (int)(key & 1ull);
-        const double gprev = gk;
         if (!flip(k, xk)) {
           failed = true;
           break;
         }
-        val += scale * gprev;
+        val += scale * gflip;
         ++nflips;
       }
       if (failed) break;
@@ -909,21 +904,13 @@ __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
           if (!((kicked[pick >> 5] >> (pick & 31)) & 1u)) break;
         }
         const int xp = (bits[pick >> 5] >> (pick & 31)) & 1;
-        // the kicked node's field, from its owner's lane
-        const int owner = (pick >> 2) & (TM_BT - 1);
-        if (warp == owner >> 5) {
-          const int s = 4 * (pick / 512) + (pick & 3);
-          const double y = tm_ld_f64(c.tbase + 2u * s);
-          if (lane == (owner & 31)) s_pub = y;
-        }
-        __syncthreads();  // everyone has read bit, field and kicked set before they change
-        const double gp = xp ? s_pub : -s_pub;
+        __syncthreads();  // everyone has read bit and kicked set before they change
         if (t == 0) kicked[pick >> 5] |= 1u << (pick & 31);
         if (!flip(pick, xp)) {
           failed = true;
           break;
         }
-        val += scale * gp;
+        val += scale * gflip;  // float64 gain of the kicked node
         ++nflips;
       }
     }
