@@ -712,9 +712,10 @@ __device__ __forceinline__ void tm_pass(const TmCtx& c, int k, int xk,
         if ((unsigned)(k - v0) < 4u) c.bits[k >> 5] ^= 1u << (k & 31);
       }
       const uint32_t nib = c.bits[v0 >> 5] >> (v0 & 31);
+      const bool full = v0 + 3 < n;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        if (v0 + i < n) {
+        if (full || v0 + i < n) {
           const int s = 8 * jj + 2 * i;
           double y = __hiloint2double((int)r[s + 1], (int)r[s]);
           if (UPD) {
