@@ -238,6 +238,37 @@ def test_errors_are_reported_and_context_survives():
     torch.cuda.synchronize()
 
 
+@pytest.mark.parametrize("n", [2, 3, 17, 100, 1023, 1025, 4097])
+@pytest.mark.parametrize("kind", ["int", "float"])
+def test_double_flips_odd_sizes(n, kind, oracle_mod):
+    """The double pass at sizes that leave partial row groups, partial column
+    chunks and fewer tiles than CTAs (each CTA streams one contiguous run of
+    tiles): its selection against the reference's fold over every pair value
+    float(g_k + g_l -/+ 2 W_kl), taken in float64 from the device's own gains,
+    for integer (int8) and float32 weights, both objectives."""
+    O = oracle_mod
+    rng = np.random.default_rng(1000 + n)
+    if kind == "int":
+        U = np.triu(rng.integers(-3, 4, size=(n, n)).astype(np.float32), 1)
+    else:
+        U = np.triu(rng.standard_normal((n, n)).astype(np.float32), 1)
+    W = U + U.T
+    th = rng.random(n) < 0.5
+    dg = _graph(W)
+    assert dg.is_integer == (kind == "int")
+    words = dg.pack(th)
+    _, g64 = dg.gains(words)
+    g = g64.cpu().numpy()
+    k, l = np.triu_indices(n, 1)
+    vals = (g[k] + g[l]) - np.where(th[k] == th[l], 2.0, -2.0) * W[k, l].astype(np.float64)
+    G, L = O.flip_geometry(n, 148)
+    for spin in (0, 1):
+        v32 = vals.astype(np.float32) * np.float32(2.0 if spin else 1.0)
+        ke, ki = O.select(v32, G, L)
+        be, bi = dg.double_bit_flips(words, g64, spin, G, L)
+        assert (float(be.item()), int(bi.item())) == (float(ke), int(ki))
+
+
 @pytest.mark.parametrize("mpe", [148, 4096])
 def test_double_flips_wide_geometry(mpe, oracle_mod):
     """n = 2200 with integer weights (exact pair values): the pair scan's
