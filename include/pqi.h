@@ -382,9 +382,10 @@ pqi_status pqi_batch_set_staging(int on);
 
 /* Tuning / cross-check knob (no reference counterpart): on (default) lets
  * pqi_batch_search (float64 local fields, CTA form) keep the fields of float
- * graphs of 4097 to 8192 nodes in tensor memory, four tasks per SM, each
- * flip's row fetched whole by one bulk copy; off keeps them in shared memory
- * (three tasks per SM). Results are identical. */
+ * graphs of 4097 to 16384 nodes in tensor memory (four tasks per SM up to 8192
+ * nodes, two up to 16384), each flip's row fetched whole by one bulk copy; off
+ * keeps them in shared memory (three tasks per SM up to 8192 nodes, one up to
+ * 16384). Results are identical. */
 pqi_status pqi_batch_set_tmem_fields(int on);
 
 /* Cross-check knob (no reference counterpart): on (default) the batched

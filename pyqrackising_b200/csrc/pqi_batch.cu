@@ -632,28 +632,38 @@ __global__ void __launch_bounds__(BT, (F32 ? 4 : 3) * 256 / BT) batch_search_ker
 }
 
 // ---------------------------------------------------------------------------
-// Float64 local fields in tensor memory (float weights, 4096 < n <= 8192).
+// Float64 local fields in tensor memory (float weights, 4096 < n <= 16384).
 //
 // The shared-memory form holds a task's float64 fields in shared memory:
 // 64 KB at n = 8192, three tasks per SM, and each flip streams its 32 KB row in
 // two register chunks. Here the fields live in the SM's tensor memory (TMEM,
-// 128 lanes x 512 columns of 32 bits): a CTA of 128 threads allocates 128
-// columns, thread t keeps its 64 nodes' fields in its own lane (node
-// v = 4 t + 512 j + i at columns 2 (4 j + i) and 2 (4 j + i) + 1), four tasks
-// per SM share the 512 columns, and shared memory is left for the flipped row:
+// 128 lanes x 512 columns of 32 bits): a CTA of 128 threads allocates 8 J
+// columns, thread t keeps its 4 J nodes' fields in its own lane (node
+// v = 4 t + 512 j + i at columns 2 (4 j + i) and 2 (4 j + i) + 1), 512 / 8 J
+// tasks per SM share the columns, and shared memory is left for the row:
 // one bulk copy of the whole row per flip (mbarrier completion). A flip pass
 // moves the fields through registers 32 columns (16 nodes) at a time with
 // tcgen05.ld / tcgen05.st; the arithmetic, the selection (float gain, lowest
 // node, the node's bit) and the float64 running value are those of the
 // shared-memory form, so both return the same states, values and flip counts.
-// Each CTA asks for enough shared memory that a fifth CTA cannot join an SM
-// whose TMEM four CTAs hold.
+// Each CTA asks for enough shared memory that no further CTA can join an SM
+// whose TMEM the resident CTAs hold.
+// The shape per J (groups of four nodes per thread): J = 16 serves n <= 8192
+// (128 columns, four CTAs per SM), J = 32 serves n <= 16384 (256 columns, two
+// CTAs per SM, where the fields in shared memory leave one).
 constexpr int TM_BT = 128;
-constexpr int TM_J = 16;                         // groups of four nodes per thread
-constexpr int TM_NMAX = 4 * TM_BT * TM_J;        // 8192 nodes
-constexpr int TM_COLS = 2 * 4 * TM_J;            // 128 columns per CTA
-constexpr int TM_STAGE_BYTES = TM_NMAX * 4;      // one float32 row
-constexpr int TM_SMEM_MIN = 50 * 1024;           // > 228 KB / 5: at most four CTAs per SM
+template <int J>
+struct TmShape {
+  static constexpr int NMAX = 4 * TM_BT * J;      // nodes
+  static constexpr int COLS = 2 * 4 * J;          // TMEM columns per CTA
+  static constexpr int CTAS = 512 / COLS;         // CTAs sharing an SM's columns
+  static constexpr int STAGE_BYTES = NMAX * 4;    // one float32 row
+  // shared memory per CTA: the stage, bits and kicked set, and at least
+  // enough that a further CTA cannot join an SM whose TMEM is taken
+  static constexpr int SMEM = (228 * 1024) / (CTAS + 1) + 4096 > STAGE_BYTES + NMAX / 4
+                                  ? (228 * 1024) / (CTAS + 1) + 4096
+                                  : STAGE_BYTES + NMAX / 4;
+};
 
 __device__ __forceinline__ void tm_st32(uint32_t taddr, const uint32_t (&r)[32]) {
   asm volatile(
@@ -688,7 +698,7 @@ struct TmCtx {
 // *out_gk the exact gain of k before the flip (its field is unchanged by its
 // own flip, W_kk = 0: the owner warp reads it back once instead of every
 // thread keeping the field of its best node); then the CTA's best key.
-template <bool UPD>
+template <bool UPD, int J>
 __device__ __forceinline__ void tm_pass(const TmCtx& c, int k, int xk,
                                         unsigned long long (*red_key)[4], double* s_yk, int par,
                                         unsigned long long* out_key, double* out_gk) {
@@ -697,7 +707,7 @@ __device__ __forceinline__ void tm_pass(const TmCtx& c, int k, int xk,
   float bv = -INFINITY;
   int bi = -1;
 #pragma unroll 1
-  for (int q = 0; q < TM_J / 4; ++q) {
+  for (int q = 0; q < J / 4; ++q) {
     if (2048 * q >= n) break;  // (uniform: no node of this chunk below n)
     uint32_t r[32];
     tc::tmem_load32(c.tbase + 32u * q, r);
@@ -754,7 +764,8 @@ __device__ __forceinline__ void tm_pass(const TmCtx& c, int k, int xk,
   if (UPD) *out_gk = xk ? s_yk[par] : -s_yk[par];
 }
 
-__global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
+template <int J>
+__global__ void __launch_bounds__(TM_BT, TmShape<J>::CTAS) batch_search_tmem_kernel(
     const BatchGraph* __restrict__ graphs, const int* __restrict__ task_graph,
     const uint32_t* __restrict__ init_states, int words_pitch, int tasks, int spin, int rounds,
     int kick, int flip_budget, uint64_t seed, const double* __restrict__ kick_cdf,
@@ -769,12 +780,13 @@ __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
   __shared__ uint32_t s_tmem;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   float* stage = reinterpret_cast<float*>(tm_smem);
-  uint32_t* bits = reinterpret_cast<uint32_t*>(tm_smem + TM_STAGE_BYTES);
-  uint32_t* kicked = bits + TM_NMAX / 32;
+  typedef TmShape<J> SH;
+  uint32_t* bits = reinterpret_cast<uint32_t*>(tm_smem + SH::STAGE_BYTES);
+  uint32_t* kicked = bits + SH::NMAX / 32;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      tc::smem_u32(&s_tmem)),
-                 "r"(TM_COLS)
+                 "r"(SH::COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
@@ -807,7 +819,7 @@ __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
     const double* __restrict__ yrow =
         (start_fields && !G.adj_ptr) ? start_fields + (size_t)task * fields_pitch : nullptr;
 #pragma unroll 1
-    for (int q = 0; q < TM_J / 4; ++q) {
+    for (int q = 0; q < J / 4; ++q) {
       uint32_t r[32];
 #pragma unroll
       for (int s = 0; s < 16; ++s) {
@@ -866,11 +878,11 @@ __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
       ok = __syncthreads_and(ok ? 1 : 0) != 0;
       phase ^= 1u;
       if (!ok) return false;
-      tm_pass<true>(c, k, xk, red_key, s_yk, par, &key, &gflip);
+      tm_pass<true, J>(c, k, xk, red_key, s_yk, par, &key, &gflip);
       par ^= 1;
       return true;
     };
-    tm_pass<false>(c, -1, 0, red_key, s_yk, par, &key, &gflip);
+    tm_pass<false, J>(c, -1, 0, red_key, s_yk, par, &key, &gflip);
     par ^= 1;
     for (int r = 0; r <= rounds && !failed; ++r) {
       for (int f = 0;; ++f) {
@@ -926,7 +938,7 @@ __global__ void __launch_bounds__(TM_BT, 4) batch_search_tmem_kernel(
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(TM_COLS)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(SH::COLS)
                  : "memory");
   }
 }
@@ -1234,25 +1246,33 @@ static pqi_status batch_search_impl(const void* graphs, int num_graphs, const in
   pqi_status sfst = start_fields(gd, task_graph, init_states, words_pitch, tasks, max_n, i8, s, &sf,
                                  &sf_pitch);
   if (sfst != PQI_OK) return sfst;
-  // float weights with float64 fields and 4096 < n <= 8192: the fields in
-  // tensor memory (four tasks per SM, each flip's whole row in one bulk copy)
-  if (!i8 && !f32 && bt == 256 && max_n > 4096 && max_n <= TM_NMAX && sf && !g_batch_no_tmem) {
-    const size_t tsm = std::max((size_t)TM_SMEM_MIN, (size_t)TM_STAGE_BYTES + TM_NMAX / 4);
-    PQI_TRY(cudaFuncSetAttribute(batch_search_tmem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)tsm));
-    PQI_TRY(cudaFuncSetAttribute(batch_search_tmem_kernel,
-                                 cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-    // resident CTAs per SM: four by shared memory and registers, and four
-    // allocations of TM_COLS fill the 512 TMEM columns (the occupancy query
+  // float weights with float64 fields and 4096 < n <= 16384: the fields in
+  // tensor memory (four tasks per SM up to 8192 nodes, two up to 16384; each
+  // flip's whole row in one bulk copy)
+  if (!i8 && !f32 && bt == 256 && max_n > 4096 && max_n <= TmShape<32>::NMAX && sf &&
+      !g_batch_no_tmem) {
+    const bool small = max_n <= TmShape<16>::NMAX;
+    const void* fn = small ? (const void*)batch_search_tmem_kernel<16> : (const void*)batch_search_tmem_kernel<32>;
+    const int tsm = small ? TmShape<16>::SMEM : TmShape<32>::SMEM;
+    PQI_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, tsm));
+    PQI_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+    // resident CTAs per SM: as many as the TMEM columns serve (shared memory
+    // and registers allow them, and keep out one more; the occupancy query
     // reports one CTA per SM for a kernel that allocates tensor memory)
     int tper = 0;
-    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tper, batch_search_tmem_kernel, TM_BT, tsm));
+    PQI_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tper, fn, TM_BT, tsm));
     if (tper >= 1) {
-      tper = 512 / TM_COLS;
+      tper = small ? TmShape<16>::CTAS : TmShape<32>::CTAS;
       const int grid = std::max(1, std::min(tasks, num_sms * tper));
-      batch_search_tmem_kernel<<<grid, TM_BT, tsm, s>>>(
-          gd, task_graph, init_states, words_pitch, tasks, is_spin_glass, rounds, kick, flip_budget,
-          seed, kick_cdf, cdf_offset, best_states, best_values, flips_total, status, sf, sf_pitch);
+      if (small) {
+        batch_search_tmem_kernel<16><<<grid, TM_BT, tsm, s>>>(
+            gd, task_graph, init_states, words_pitch, tasks, is_spin_glass, rounds, kick, flip_budget,
+            seed, kick_cdf, cdf_offset, best_states, best_values, flips_total, status, sf, sf_pitch);
+      } else {
+        batch_search_tmem_kernel<32><<<grid, TM_BT, tsm, s>>>(
+            gd, task_graph, init_states, words_pitch, tasks, is_spin_glass, rounds, kick, flip_budget,
+            seed, kick_cdf, cdf_offset, best_states, best_values, flips_total, status, sf, sf_pitch);
+      }
       PQI_LAUNCHED("batch_search_tmem_kernel");
       PQI_TRY(cudaFreeAsync(sf, s));
       return PQI_OK;

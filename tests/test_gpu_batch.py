@@ -306,19 +306,21 @@ def test_float32_fields_staged_rows_match_register_rows():
         assert np.all(x * (W @ x) <= 1e-5 * np.abs(W).sum(axis=1).max())
 
 
-def test_tmem_fields_match_shared_memory_fields():
+@pytest.mark.parametrize("sizes", [(8192, 5000, 4500), (12000, 9000, 8300)])
+def test_tmem_fields_match_shared_memory_fields(sizes):
     """Float64 fields in tensor memory (float graphs of 4097-8192 nodes, four
-    tasks per SM) give the same states, values and flip counts as the fields
-    in shared memory, for dense graphs (starting fields from the start pass)
-    and row-list graphs (summed by each field's owner), with kicks; the states
-    are local optima of the float64 objective."""
+    tasks per SM; 8193-16384 nodes, two) give the same states, values and flip
+    counts as the fields in shared memory, for dense graphs (starting fields
+    from the start pass) and row-list graphs (summed by each field's owner),
+    with kicks; the values are the float64 objective of the states."""
     from pyqrackising_b200 import _lib
     from pyqrackising_b200 import workloads as wl
     from pyqrackising_b200.batch import BatchedSearch
     from pyqrackising_b200.device import DeviceGraph
 
-    Ws = [wl.sherrington_kirkpatrick(8192, seed=31), wl.gnp_weighted(5000, 0.02, seed=32, dist="normal"),
-          wl.gnp_weighted(4500, 0.3, seed=33, dist="uniform")]
+    n0, n1, n2 = sizes
+    Ws = [wl.sherrington_kirkpatrick(n0, seed=31), wl.gnp_weighted(n1, 0.02, seed=32, dist="normal"),
+          wl.gnp_weighted(n2, 0.3, seed=33, dist="uniform")]
     bs = BatchedSearch([DeviceGraph(W) for W in Ws])
     task_graph = [0, 1, 2, 0, 1, 2, 0]
     words = bs.random_states(task_graph, seed=8)
